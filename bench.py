@@ -1,0 +1,444 @@
+"""PBF step benchmark on B200 (one JSON line on stdout from rank 0).
+
+Workload (default): the 1,003,520-particle dam break in an 86h cube box
+(636,056 hash cells), 5 solver iterations, dt = 1/120 s, seeded jittered
+lattice (synthetic; see mtlphys_b200/configs.py).  A "step" is one full PBF
+step: predict, spatial hash, K x (lambda, delta), scatter-back, finalize,
+foam.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value          ms per 1M-particle step for the whole job: device time (CUDA
+               events on the engine's stream, L2 flushed between timed steps,
+               max over ranks) / (K * N).  N > 1 runs N independent replicas
+               (a single scene does not shard: no data-path collective).
+e2e            the same metric through the C ABI with the state in pinned
+               host memory: every step uploads positions + velocities, steps,
+               and downloads them.
+roofline       the dominant kernel's algorithmic bytes per launch / its mean
+               CUDA-event duration, against the measured HBM copy bandwidth.
+cpu_baseline   the FP64 oracle (OpenMP on the host cores) on a bounded
+               sample of the same workload (rank 0, N = 1).
+--impl reference  the reference's own compute shaders compiled as C++
+               (oracle/_ref; OpenMP on all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PBF step ms @1M (%HBM peak); batched vs serial scenes/s; adjoint/fwd ratio"
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 256 << 20
+
+
+# ---- algorithmic bytes (reference dataflow, each array element read or written
+# once per reference kernel that touches it) --------------------------------------
+def kernel_bytes(n: int, c: int) -> dict:
+    """Bytes per launch of each kernel of this engine, as the sum of the
+    reference kernels it replaces (predict 64N, hash 20N, count 4N+8C, zero
+    8C, scan 16C, scatter 8N+12C, gather 36N, countNeighbors 40N+4C, lambda
+    28N+4C, delta 36N+4C, scatter-back 36N, finalize 64N, foam 24N)."""
+    return {
+        "predict_hash": 88 * n + 8 * c,
+        "scan": 24 * c,
+        "scatter": 8 * n + 12 * c,
+        "sort_gather": 36 * n,
+        "long_segments": 0,
+        "lambda_count": 68 * n + 8 * c,
+        "lambda": 28 * n + 4 * c,
+        "delta": 36 * n + 4 * c,
+        "delta_finalize": 160 * n + 4 * c,
+    }
+
+
+def step_bytes(n: int, c: int, k: int) -> int:
+    return (296 + 64 * k) * n + (48 + 8 * k) * c
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---- clocks ------------------------------------------------------------------------
+REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(REASONS, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- distributed plumbing ----------------------------------------------------------
+def dist_setup(n_gpus: int):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def gpu_uuid(local: int) -> str:
+    import torch
+
+    try:
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else f"GPU-{u}"
+    except Exception:
+        return str(local)
+
+
+# ---- our arm -------------------------------------------------------------------------
+def run_ours(args, world, rank, local) -> dict | None:
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from mtlphys_b200 import Engine, _abi, configs
+
+    w = configs.WORKLOADS[args.workload]()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    e = Engine(local)
+    e.set_params(w.params)
+    e.reset(w.n, w.scene, w.desc)
+    n, k_it = w.n, int(w.params.solver_iterations)
+    cells = e.total_cells()
+    e.set_graph_mode(True)
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+
+    for _ in range(args.warmup):
+        e.step(w.dt, stream)
+    stream.synchronize()
+    if e.check_errors():
+        raise RuntimeError("device error during warm-up")
+
+    # ---- timed region: K steps, L2 flushed between steps (outside the events)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    dist_barrier(world)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(gpu_uuid(local)) as clk:
+        for i in range(args.steps):
+            flush_l2()
+            starts[i].record(stream)
+            e.step(w.dt, stream)
+            ends[i].record(stream)
+        torch.cuda.synchronize(dev)
+    dist_barrier(world)
+    total_ms = sum(s.elapsed_time(t) for s, t in zip(starts, ends))
+    e.check_errors()
+    total_ms = dist_max(total_ms, world)
+    ms_per_step = total_ms / args.steps
+    value = total_ms / (args.steps * world)
+
+    # ---- hot-L2 steady state (back-to-back steps, for reference only)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e.step(w.dt, stream)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    hot_ms = ev0.elapsed_time(ev1) / args.steps
+
+    # ---- per-kernel timing (CUDA events around every launch, L2 flushed)
+    e.set_graph_mode(False)
+    e.set_profiling(True)
+    e.kernel_times()
+    prof_steps = max(3, min(args.steps, 10))
+    for _ in range(prof_steps):
+        flush_l2()
+        e.step(w.dt, stream)
+    times = e.kernel_times()
+    e.set_profiling(False)
+    kb = kernel_bytes(n, cells)
+    kernels = {}
+    for name, (launches, ms) in times.items():
+        avg = ms / max(1, launches)
+        gbs = kb.get(name, 0) / (avg * 1e-3) / 1e9 if avg > 0 else 0.0
+        kernels[name] = {"launches_per_step": launches / prof_steps, "ms": round(avg, 5),
+                         "algorithmic_bytes": kb.get(name, 0), "GB/s": round(gbs, 1)}
+    dominant = max(kernels, key=lambda k: kernels[k]["ms"] * kernels[k]["launches_per_step"])
+    peak, peak_kind = measured_hbm_peak()
+    dk = kernels[dominant]
+    traffic = read_traffic(dominant)
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["GB/s"], "peak": peak,
+                "unit": "GB/s", "frac": round(dk["GB/s"] / peak, 4), "traffic": traffic,
+                "peak_source": peak_kind,
+                "step_frac": round(step_bytes(n, cells, k_it) / (ms_per_step * 1e-3) / 1e9 / peak, 4)}
+
+    # ---- end to end through the C ABI with host (pinned) buffers
+    lib = _abi.load()
+    h_pos = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    h_vel = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    sh = C.c_void_p(stream.cuda_stream)
+    _abi.check(lib.mp_engine_download(e._h, _abi.MP_BUF_POSITIONS, C.c_void_p(h_pos.data_ptr()), n, sh), "download")
+    _abi.check(lib.mp_engine_download(e._h, _abi.MP_BUF_VELOCITIES, C.c_void_p(h_vel.data_ptr()), n, sh), "download")
+    e.set_graph_mode(True)
+    e2e_steps = max(3, args.steps // 2)
+
+    def e2e_step():
+        _abi.check(lib.mp_engine_upload(e._h, _abi.MP_BUF_POSITIONS, C.c_void_p(h_pos.data_ptr()), n, sh), "upload")
+        _abi.check(lib.mp_engine_upload(e._h, _abi.MP_BUF_VELOCITIES, C.c_void_p(h_vel.data_ptr()), n, sh), "upload")
+        _abi.check(lib.mp_engine_step(e._h, C.c_float(w.dt), sh), "step")
+        _abi.check(lib.mp_engine_download(e._h, _abi.MP_BUF_POSITIONS, C.c_void_p(h_pos.data_ptr()), n, sh), "download")
+        _abi.check(lib.mp_engine_download(e._h, _abi.MP_BUF_VELOCITIES, C.c_void_p(h_vel.data_ptr()), n, sh), "download")
+
+    e2e_step()
+    dist_barrier(world)
+    torch.cuda.synchronize(dev)
+    e2e_ms = 0.0
+    for _ in range(e2e_steps):
+        flush_l2()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        e2e_step()
+        s1.record(stream)
+        s1.synchronize()
+        e2e_ms += s0.elapsed_time(s1)
+    e.check_errors()
+    e2e_ms = dist_max(e2e_ms, world)
+    e2e_value = e2e_ms / (e2e_steps * world)
+    e.close()
+
+    if rank != 0:
+        return None
+    line = {
+        "metric": METRIC, "value": round(value, 5), "unit": "ms/step", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded jittered lattice (dam break), no dataset",
+        "config": {**w.describe(), "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed between timed steps (256 MiB write outside the events)",
+                   "mode": "CUDA graph replay of the step"},
+        "ms_per_step_hot_l2": round(hot_ms, 5),
+        "steps_per_s": round(1000.0 / ms_per_step, 2),
+        "particle_steps_per_s": round(n * world * 1000.0 / ms_per_step, 1),
+        "roofline": roofline, "kernels": kernels,
+        "e2e": {"value": round(e2e_value, 5), "unit": "ms/step", "h2d_bytes_per_step": 32 * n,
+                "d2h_bytes_per_step": 32 * n, "steps": e2e_steps},
+        "gpu_launches": int(lib.mp_step_launch_count(k_it)) * args.steps,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, args)
+    return line
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel:
+                    return int(float(parts[1]))
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(w, args) -> dict:
+    """The FP64 oracle on the host cores, a bounded sample of the workload."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    pos = O.seed_scene(w.params, w.scene, w.n, w.desc)
+    vel = np.zeros_like(pos)
+    O.set_threads(0)
+    steps = 0
+    t0 = time.perf_counter()
+    while steps < args.cpu_steps and (time.perf_counter() - t0) < args.cpu_budget_s:
+        o = O.step(w.params, w.dt, pos, vel)
+        pos = np.concatenate([o["pos"], np.ones((w.n, 1))], axis=1).astype(np.float32)
+        vel = np.concatenate([o["vel"], np.zeros((w.n, 1))], axis=1).astype(np.float32)
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": round(dt * 1000.0 / steps, 2), "unit": "ms/step", "cores": O.threads(),
+            "kind": "port",
+            "sample": f"first {steps} steps of the {w.name} workload ({w.n} particles), FP64 oracle"}
+
+
+# ---- reference arm ----------------------------------------------------------------------
+def run_reference(args, world, rank) -> dict | None:
+    if rank != 0:
+        return None
+    import numpy as np
+
+    from mtlphys_b200 import configs
+    from oracle import oracle as O
+
+    w = configs.WORKLOADS[args.workload]()
+    cores = os.cpu_count() or 1
+    pos = O.seed_scene(w.params, w.scene, w.n, w.desc)
+    vel = np.zeros_like(pos)
+    if O.has_ref():
+        kind = "reference"
+        O.ref_set_threads(cores)
+        p = w.params.copy()
+
+        def step(pos, vel):
+            o = O.ref_step(p, w.dt, pos, vel)
+            return o["pos"], o["vel"]
+        what = ("the reference's compute shaders (engine/shaders/*.metal) compiled as C++, "
+                "dispatched in Engine::step order; s_corr k is the shaders' hard-coded 1e-4")
+    else:
+        kind = "port"
+        O.set_threads(cores)
+
+        def step(pos, vel):
+            o = O.step(w.params, w.dt, pos, vel)
+            return (np.concatenate([o["pos"], np.ones((w.n, 1))], axis=1).astype(np.float32),
+                    np.concatenate([o["vel"], np.zeros((w.n, 1))], axis=1).astype(np.float32))
+        what = "FP64 oracle port"
+    for _ in range(min(args.warmup, 2)):
+        pos, vel = step(pos, vel)
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < args.steps and (steps == 0 or time.perf_counter() - t0 < args.cpu_budget_s):
+        pos, vel = step(pos, vel)
+        steps += 1
+    ms = (time.perf_counter() - t0) * 1000.0 / steps
+    return {
+        "metric": METRIC, "value": round(ms, 3), "unit": "ms/step", "impl": "reference",
+        "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 2), "ms_per_step": round(ms, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded jittered lattice (dam break), no dataset",
+        "config": {**w.describe(), "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms/step", "cores": cores, "kind": kind,
+                         "sample": f"{steps} steps of {w.name} ({w.n} particles): {what}"},
+        "e2e": {"value": round(ms, 3), "unit": "ms/step", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["dam_break", "cube_drop"], default="dam_break")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-budget-s", type=float, default=60.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("--warmup must be >= 3")
+
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        line = run_reference(args, world, rank)
+    else:
+        world, rank, local = dist_setup(args.gpus)
+        line = run_ours(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,225 @@
+/*
+ * mtlphys_b200.h — C ABI of the B200 Position-Based Fluids engine.
+ *
+ * This is the drop-in boundary for the simulation step of the reference
+ * engine.  Every entry point below replaces one member of the reference's
+ * C++ `mtlphys::Engine` class (engine/include/mtlphys/Engine.hpp) or one
+ * method of its Obj-C++ bridge (app/bridge/EngineBridge.h); the citation is
+ * given beside each declaration.
+ *
+ * Conventions
+ *  - Every call returns an int status: MP_OK (0) or one of MP_ERR_*.  The
+ *    reference aborts on fatal errors (engine/src/Engine.cpp:72-83, 407-413,
+ *    849-854); this ABI returns a status instead and keeps a per-thread
+ *    message readable with mp_last_error().
+ *  - The engine owns its device buffers (like the reference owns its
+ *    MTL::Buffer objects).  mp_engine_buffer() hands out borrowed device
+ *    pointers; mp_engine_upload()/mp_engine_download() copy host data.
+ *  - GPU work is enqueued asynchronously on the caller's CUDA stream
+ *    (`mp_stream`, a cudaStream_t passed as void*; NULL = legacy default
+ *    stream).  This replaces the caller-supplied MTL::CommandBuffer of the
+ *    reference: step() only encodes, the caller decides when to wait.
+ *    Only download, mp_engine_synchronize and mp_engine_check_errors block.
+ *  - Not thread-safe: one host thread per engine (Engine.hpp:4-6).
+ *  - Particle state is float4 per particle (x, y, z, w) in original
+ *    particle order, as the reference's positions/velocities buffers.
+ */
+#ifndef MTLPHYS_B200_H
+#define MTLPHYS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define MP_OK                    0
+#define MP_ERR_INVALID_ARGUMENT  1   /* bad handle, size, scene id, ...        */
+#define MP_ERR_OUT_OF_MEMORY     2   /* device or host allocation failed       */
+#define MP_ERR_CUDA              3   /* a CUDA runtime call failed             */
+#define MP_ERR_DEVICE            4   /* a kernel set the device error word     */
+#define MP_ERR_SPIN_LIMIT        5   /* a bounded device-side wait gave up     */
+#define MP_ERR_UNSUPPORTED       6   /* feature not available in this build    */
+
+/* bits of the device error word (mp_engine_check_errors) */
+#define MP_DEVERR_SPIN_LIMIT     0x1u  /* scan look-back / grid barrier timed out */
+#define MP_DEVERR_NAN            0x2u  /* a non-finite position left a step       */
+#define MP_DEVERR_INDEX          0x4u  /* an index check failed (debug checks)    */
+
+/* ---- scenes: Engine.hpp:37-39 ------------------------------------------- */
+#define MP_SCENE_CUBE_DROP    0u
+#define MP_SCENE_DAM_BREAK    1u
+#define MP_SCENE_SPHERE_DROP  2u
+
+/* ---- buffers: Engine.hpp:83-90 accessors (+ foam, sorted state) --------- */
+#define MP_BUF_POSITIONS        0u  /* float4[N]  positionsBuffer()      */
+#define MP_BUF_VELOCITIES       1u  /* float4[N]  velocitiesBuffer()     */
+#define MP_BUF_PREV_POSITIONS   2u  /* float4[N]  prevPositionsBuffer()  */
+#define MP_BUF_CELL_HASHES      3u  /* uint32[N]  cellHashesBuffer()     */
+#define MP_BUF_CELL_START       4u  /* uint32[C+1] cellStartBuffer()     */
+#define MP_BUF_SORTED_INDEX     5u  /* uint32[N]  sortedIndexBuffer()    */
+#define MP_BUF_NEIGHBOR_COUNTS  6u  /* uint32[N]  neighborCountsBuffer() */
+#define MP_BUF_LAMBDAS          7u  /* float[N]   lambdasBuffer()        */
+#define MP_BUF_FOAM             8u  /* float[N]   _foamIntensity         */
+#define MP_BUF_SORTED_POSITIONS 9u  /* float4[N]  _sortedPositions (hash-time gather) */
+#define MP_BUF_COUNT           10u
+
+typedef void* mp_stream;             /* cudaStream_t */
+typedef struct mp_engine mp_engine;  /* opaque */
+
+/*
+ * Simulation parameters.  The reference hard-codes these as constexpr
+ * tunables (engine/src/Engine.cpp:22-39, 551-572) and as literals inside its
+ * shaders (engine/shaders/Constraints.metal:158-160, 190, 297, 325, 341-347);
+ * here every one of them is a field.  mp_default_params() fills the
+ * reference's values.  `size` must be sizeof(mp_pbf_params).
+ */
+typedef struct mp_pbf_params {
+    uint32_t size;               /* sizeof(mp_pbf_params)                          */
+    uint32_t solver_iterations;  /* kSolverIters = 5      (Engine.cpp:39)          */
+    float    h;                  /* kSmoothingH = 0.10    (Engine.cpp:29)          */
+    float    cell_size;          /* kCellSize = 0.10      (Engine.cpp:25)          */
+    float    rest_density;       /* kRestDensity = 8000   (Engine.cpp:32)          */
+    float    epsilon;            /* kEpsilonCFM = 800     (Engine.cpp:35)          */
+    float    damping;            /* kPBFDamping = 0.996   (Engine.cpp:36)          */
+    float    gravity[3];         /* (0,-9.81,0)           (Engine.cpp:558)         */
+    float    bounds_min[3];      /* kBoundsMin (-3,-3,-3) (Engine.cpp:23)          */
+    float    bounds_max[3];      /* kBoundsMax (3,6,3)    (Engine.cpp:24)          */
+    float    scorr_k;            /* kSCorrK = 1e-4        (Constraints.metal:158)  */
+    uint32_t scorr_n;            /* ratio^4               (Constraints.metal:179)  */
+    float    scorr_dq;           /* 0.2 (x h)             (Constraints.metal:159)  */
+    float    max_delta;          /* 0.3 (x h)             (Constraints.metal:190)  */
+    float    vmax;               /* 1.0 (x h/dt)          (Constraints.metal:347)  */
+    float    wall_eps;           /* 1e-3                  (Constraints.metal:325)  */
+    float    floor_friction;     /* 0.55                  (Constraints.metal:341)  */
+    float    wall_friction;      /* 0.97                  (Constraints.metal:344)  */
+    float    foam_max_neighbors; /* kMaxNeighborsForViz=96 (Engine.cpp:27, 806)   */
+    float    foam_speed_lo;      /* 1.2                   (Constraints.metal:297)  */
+    float    foam_speed_hi;      /* 4.5                   (Constraints.metal:297)  */
+    float    sphere_radius;      /* 0.6                   (Engine.hpp:184)         */
+    float    sphere_gravity;     /* -9.81                 (Engine.cpp:694)         */
+    float    sphere_drag;        /* 0.998 per step        (Engine.cpp:695-697)     */
+    float    sphere_restitution; /* 0.4                   (Engine.cpp:702-707)     */
+} mp_pbf_params;
+
+/*
+ * Scene description for mp_engine_reset_scene().  With lattice == 0 the
+ * reference's own placement for the scene is used (Engine.cpp:454-549).
+ * With lattice == 1 particles are placed on a dims[0] x dims[1] x dims[2]
+ * lattice with lower corner `origin`, x fastest, then z, then y (the
+ * reference's loop order), each component jittered by a uniform value in
+ * [-jitter, +jitter) drawn from std::mt19937_64(seed) as
+ * ((draw >> 11) * 2^-53 * 2 - 1) * jitter, x then y then z per particle.
+ * `size` must be sizeof(mp_scene_desc).
+ */
+typedef struct mp_scene_desc {
+    uint32_t size;
+    uint32_t lattice;            /* 0: reference placement, 1: explicit lattice   */
+    uint64_t seed;               /* jitter seed                                   */
+    uint32_t dims[3];            /* lattice counts along x, y, z                  */
+    float    origin[3];          /* lattice lower corner                          */
+    float    spacing;            /* lattice spacing (0 -> 0.5 h, Engine.cpp:457)  */
+    float    jitter;             /* absolute jitter amplitude per component       */
+    float    sphere_center[3];   /* scene 2: sphere start (Engine.cpp:523-525)    */
+    float    sphere_velocity[3]; /* scene 2: sphere start velocity (0 in ref)     */
+} mp_scene_desc;
+
+/* ---- library ------------------------------------------------------------ */
+/* Last error message of the calling thread ("" if none). */
+const char* mp_last_error(void);
+/* ABI version: increases when a struct or signature changes. */
+uint32_t mp_abi_version(void);
+/* Reference defaults: Engine.cpp:22-39, 551-572; Constraints.metal literals. */
+int mp_default_params(mp_pbf_params* out);
+/* Defaults for mp_scene_desc (reference placement). */
+int mp_default_scene_desc(mp_scene_desc* out);
+/* Rest density of an interior lattice site at `spacing` for smoothing length
+ * h: FP64 sum of Poly6 over the lattice (the quantity Engine.cpp:30-31
+ * approximates as ~8072 before hard-coding 8000). */
+double mp_lattice_rest_density(double h, double spacing);
+
+/* ---- engine lifetime: Engine.hpp:29-30, 41-44 ---------------------------- */
+/* Engine(MTL::Device*) — binds `device`, then reset(200'000) like
+ * Engine.cpp:97-102. */
+int mp_engine_create(int device, mp_engine** out);
+/* ~Engine() (Engine.cpp:104-123). NULL is accepted. */
+int mp_engine_destroy(mp_engine* e);
+/* Replaces the constexpr tunables; takes effect at the next reset/step
+ * (a change of bounds or cell size re-derives the grid at the next reset). */
+int mp_engine_set_params(mp_engine* e, const mp_pbf_params* p);
+int mp_engine_get_params(const mp_engine* e, mp_pbf_params* out);
+/* reset(particleCount) — keeps the current scene (Engine.cpp:125-127). */
+int mp_engine_reset(mp_engine* e, uint32_t n);
+/* reset(particleCount, sceneIdx) (Engine.cpp:129-134); desc may be NULL. */
+int mp_engine_reset_scene(mp_engine* e, uint32_t n, uint32_t scene, const mp_scene_desc* desc);
+
+/* ---- simulation: Engine.hpp:52, 56 --------------------------------------- */
+/* step(cmd, dt): predict -> spatial hash -> K solver iterations -> scatter
+ * back -> finalize -> foam (Engine.cpp:685-811).  dt <= 0 is a no-op that
+ * returns MP_OK (Engine.cpp:686). */
+int mp_engine_step(mp_engine* e, float dt, mp_stream stream);
+/* buildSpatialHash(cmd): hash, count, scan, scatter, gather, neighbour
+ * count of the current positions (Engine.cpp:601-679).  The intra-cell
+ * order of sortedIndex is ascending particle index (deterministic). */
+int mp_engine_build_spatial_hash(mp_engine* e, mp_stream stream);
+/* Capture step() into a CUDA graph and replay it (1) or launch kernel by
+ * kernel (0, default).  Results are identical either way. */
+int mp_engine_set_graph_mode(mp_engine* e, int enable);
+
+/* ---- tracing (no reference counterpart: the reference reads only
+ *      command-buffer timestamps, tests/bench_engine.cpp:43) ---------------- */
+typedef struct mp_kernel_time {
+    char     name[32];   /* kernel kind, e.g. "lambda", "delta", "scan"   */
+    uint32_t launches;   /* launches timed since the last read            */
+    double   ms;         /* total device time of those launches           */
+} mp_kernel_time;
+/* Time every kernel the engine launches with CUDA events on its stream
+ * (1), or stop (0).  While profiling, step() runs kernel by kernel. */
+int mp_engine_set_profiling(mp_engine* e, int enable);
+/* Wait for the timed work and return per-kernel totals (up to `capacity`
+ * entries; *count = number of kernel kinds); the totals are then cleared. */
+int mp_engine_kernel_times(mp_engine* e, mp_kernel_time* out, uint32_t capacity, uint32_t* count);
+/* Kernel launches one step() issues for `iterations` solver iterations. */
+uint32_t mp_step_launch_count(uint32_t iterations);
+
+/* ---- queries: Engine.hpp:44, 78-80 --------------------------------------- */
+uint32_t mp_engine_particle_count(const mp_engine* e);
+uint32_t mp_engine_total_cells(const mp_engine* e);
+float    mp_engine_cell_size(const mp_engine* e);
+uint32_t mp_engine_current_scene(const mp_engine* e);
+/* Grid dimensions of the spatial hash (SpatialParams::gridDim, Shared.h:47). */
+int mp_engine_grid_dims(const mp_engine* e, uint32_t dims[3]);
+
+/* ---- buffers: Engine.hpp:83-90 ------------------------------------------- */
+/* Borrowed device pointer and byte size of buffer `which` (MP_BUF_*). */
+int mp_engine_buffer(mp_engine* e, uint32_t which, void** dptr, size_t* bytes);
+/* Copy `count` elements (float4, uint32 or float per the buffer's type)
+ * between host memory and buffer `which`.  upload is ordered on `stream`
+ * and returns once the host memory may be reused; download synchronizes. */
+int mp_engine_upload(mp_engine* e, uint32_t which, const void* host, size_t count, mp_stream stream);
+int mp_engine_download(mp_engine* e, uint32_t which, void* host, size_t count, mp_stream stream);
+/* Sphere state of scene 2 (Engine.hpp:182-184). */
+int mp_engine_set_sphere(mp_engine* e, const float center[3], const float velocity[3], float radius);
+int mp_engine_get_sphere(mp_engine* e, float center[3], float velocity[3], float* radius);
+/* Wait for the engine's queued work and report the device error word
+ * (MP_DEVERR_* in *bits, may be NULL); the word is cleared. */
+int mp_engine_check_errors(mp_engine* e, uint32_t* bits);
+int mp_engine_synchronize(mp_engine* e);
+
+/* ---- scan: Engine.hpp:92-100 --------------------------------------------- */
+/* runExclusiveScan(cmd, in, out, chunkSums, n) (Engine.cpp:843-882): out[i]
+ * = sum of in[0..i) modulo 2^32, single pass with decoupled look-back; no
+ * 1024^2 length cap.  `in` and `out` are device pointers; `scratch` is a
+ * device buffer of at least mp_exclusive_scan_scratch_bytes(n) bytes.
+ * n == 0 is a no-op (Engine.cpp:848).  in == out is allowed. */
+size_t mp_exclusive_scan_scratch_bytes(uint32_t n);
+int mp_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n,
+                      void* scratch, size_t scratch_bytes, mp_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MTLPHYS_B200_H */

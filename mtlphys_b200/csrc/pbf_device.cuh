@@ -1,0 +1,108 @@
+// pbf_device.cuh — device-side types and per-particle math of the PBF step.
+//
+// The arithmetic follows the reference shaders:
+//   cell coordinates / hash ........ engine/shaders/Spatial.metal:35-43
+//   poly6 / spiky gradient ......... engine/shaders/Constraints.metal:29-39
+//   lambda ......................... Constraints.metal:124-127
+//   position correction + s_corr ... Constraints.metal:170-198
+//   sphere push .................... Constraints.metal:262-277
+//   finalize ....................... Constraints.metal:305-353
+//   foam ........................... Constraints.metal:287-299
+// Every constant the reference hard-codes in a shader is a field of
+// StepConsts (filled from mp_pbf_params on the host).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpb {
+
+// Uniform hash grid: SpatialParams (engine/shaders/Shared.h:40-49).
+struct GridDev {
+    float ox, oy, oz;  // gridOrigin (= bounds_min)
+    float inv;         // invCellSize = 1.0f / cellSize, rounded on the host
+    int gx, gy, gz;    // gridDim
+    uint32_t cells;    // gx * gy * gz
+};
+
+// Per-launch constants of one step (PBFParams, Shared.h:53-71, plus the
+// shader literals).  Passed by value.
+struct StepConsts {
+    GridDev g;
+    uint32_t n;
+    float h, h2, poly6, spiky;
+    float inv_rho0, eps;
+    float scorr_k, inv_wq, max_step;
+    uint32_t scorr_n;
+    float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
+    float gravx, gravy, gravz;
+    float dt, inv_dt, damping, vmax;
+    float wall_eps, floor_fric, wall_fric;
+    float foam_maxn, foam_lo, foam_hi;
+    int sphere;  // 1: sphere-drop scene (sphere state lives in device memory)
+    float sph_gravity, sph_drag, sph_rest;
+};
+
+// Device-resident sphere state: center xyz, velocity xyz, radius.
+struct SphereState {
+    float c[3];
+    float v[3];
+    float r;
+    float pad;
+};
+
+constexpr uint32_t kDevErrSpin = 0x1u;
+constexpr uint32_t kDevErrNaN = 0x2u;
+constexpr uint32_t kDevErrIndex = 0x4u;
+
+#ifdef __CUDACC__
+// ---- spatial hash -----------------------------------------------------------
+
+// cellCoordOf: q = (p - origin) * invCellSize, floor, clamp to [0, dim-1].
+// Explicit round-to-nearest ops keep the two roundings of the reference
+// formula (no contraction), and cvt.rmi saturates (NaN -> 0) so that every
+// input maps to a valid cell.
+__device__ __forceinline__ int cell_axis(float p, float o, float inv, int dim) {
+    const float q = __fmul_rn(__fsub_rn(p, o), inv);
+    const int c = __float2int_rd(q);
+    return min(max(c, 0), dim - 1);
+}
+
+__device__ __forceinline__ uint32_t cell_hash(const GridDev& g, int x, int y, int z) {
+    return uint32_t(x) + uint32_t(y) * uint32_t(g.gx) + uint32_t(z) * uint32_t(g.gx) * uint32_t(g.gy);
+}
+
+__device__ __forceinline__ void cell_of(const GridDev& g, float px, float py, float pz, int& cx,
+                                        int& cy, int& cz) {
+    cx = cell_axis(px, g.ox, g.inv, g.gx);
+    cy = cell_axis(py, g.oy, g.inv, g.gy);
+    cz = cell_axis(pz, g.oz, g.inv, g.gz);
+}
+
+// Squared distance with one fixed rounding order, shared by the neighbour
+// count and the solver so that integer outputs are reproducible.
+__device__ __forceinline__ float dist2(float dx, float dy, float dz) {
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+// ---- SPH kernels ------------------------------------------------------------
+
+__device__ __forceinline__ float pow_n(float x, uint32_t n) {
+    if (n == 4u) {
+        const float x2 = x * x;
+        return x2 * x2;
+    }
+    float r = 1.0f;
+    for (uint32_t e = 0; e < n; ++e) r *= x;
+    return r;
+}
+
+__device__ __forceinline__ float smoothstep_f(float e0, float e1, float x) {
+    float t = (x - e0) / (e1 - e0);
+    t = fminf(fmaxf(t, 0.0f), 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
+#endif  // __CUDACC__
+
+}  // namespace mpb

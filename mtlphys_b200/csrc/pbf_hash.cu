@@ -1,0 +1,413 @@
+// pbf_hash.cu — spatial hash of the PBF step for sm_100a.
+//
+// Replaces the reference's hash pipeline (engine/shaders/Spatial.metal:49-243,
+// dispatched by engine/src/Engine.cpp:601-679):
+//   predict + hash + count  one pass; warp-aggregated atomics (__match_any_sync)
+//                           hand each particle its rank among the particles of
+//                           its cell that this pass saw
+//   exclusive scan          single pass, decoupled look-back, warp shuffles
+//                           (replaces scanChunkExclusive/scanChunkSums/
+//                           addChunkOffsets and their 1024^2 cap); also zeroes
+//                           the counts for the next pass
+//   scatter                 slot = cellStart[c] + rank (no second atomic)
+//   stable fix-up + gather  re-ranks each particle inside its cell segment by
+//                           particle index, so sortedIndex is ascending within a
+//                           cell (deterministic, unlike scatterParticles'
+//                           atomics), and gathers the sorted positions
+//   countNeighbors          only for the standalone buildSpatialHash; the step
+//                           fuses the count into its first lambda pass.
+#include "pbf_kernels.h"
+
+namespace mpb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait (~0.1-1 s)
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Engine.cpp:694-707 (host-side sphere kinematics in the reference), in FP32
+// with one rounding per operation, run by one thread before the hash.
+__device__ void sphere_advance(const StepConsts& c, SphereState* s) {
+    float vx = s->v[0], vy = s->v[1], vz = s->v[2];
+    vy = __fadd_rn(vy, __fmul_rn(c.sph_gravity, c.dt));
+    vx = __fmul_rn(vx, c.sph_drag);
+    vy = __fmul_rn(vy, c.sph_drag);
+    vz = __fmul_rn(vz, c.sph_drag);
+    float p[3] = {__fadd_rn(s->c[0], __fmul_rn(vx, c.dt)), __fadd_rn(s->c[1], __fmul_rn(vy, c.dt)),
+                  __fadd_rn(s->c[2], __fmul_rn(vz, c.dt))};
+    float v[3] = {vx, vy, vz};
+    const float lo[3] = {c.bminx, c.bminy, c.bminz};
+    const float hi[3] = {c.bmaxx, c.bmaxy, c.bmaxz};
+    const float r = s->r;
+    for (int a = 0; a < 3; ++a) {
+        if (__fsub_rn(p[a], r) < lo[a]) {
+            p[a] = __fadd_rn(lo[a], r);
+            v[a] = __fmul_rn(-v[a], c.sph_rest);
+        }
+        if (__fadd_rn(p[a], r) > hi[a]) {
+            p[a] = __fsub_rn(hi[a], r);
+            v[a] = __fmul_rn(-v[a], c.sph_rest);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        s->c[a] = p[a];
+        s->v[a] = v[a];
+    }
+}
+
+// predictPositions (Constraints.metal:54-66) + hashCells (Spatial.metal:49-57)
+// + countCells (Spatial.metal:63-70) in one pass.
+__global__ void __launch_bounds__(256)
+k_predict_hash(StepConsts c, float4* __restrict__ pos, const float4* __restrict__ vel,
+               float4* __restrict__ prev, uint32_t* __restrict__ hash, uint32_t* __restrict__ off,
+               uint32_t* __restrict__ counts, uint32_t* __restrict__ long_count,
+               SphereState* __restrict__ sphere, int predict) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *long_count = 0;
+        if (predict && c.sphere) sphere_advance(c, sphere);
+    }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < c.n;
+    uint32_t cell = 0;
+    if (active) {
+        float4 p = pos[i];
+        if (predict) {
+            const float4 v = vel[i];
+            prev[i] = p;
+            // v' = v + g*dt and p' = p + v'*dt, each one fused multiply-add.
+            const float vx = __fmaf_rn(c.gravx, c.dt, v.x);
+            const float vy = __fmaf_rn(c.gravy, c.dt, v.y);
+            const float vz = __fmaf_rn(c.gravz, c.dt, v.z);
+            p.x = __fmaf_rn(vx, c.dt, p.x);
+            p.y = __fmaf_rn(vy, c.dt, p.y);
+            p.z = __fmaf_rn(vz, c.dt, p.z);
+            pos[i] = p;
+        }
+        int cx, cy, cz;
+        cell_of(c.g, p.x, p.y, p.z, cx, cy, cz);
+        cell = cell_hash(c.g, cx, cy, cz);
+        hash[i] = cell;
+    }
+    // Warp-aggregated count: one atomic per distinct cell in the warp.
+    const unsigned act = __ballot_sync(kFull, active);
+    if (active) {
+        const unsigned peers = __match_any_sync(act, cell);
+        const int leader = __ffs(peers) - 1;
+        const int lane = threadIdx.x & 31;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(&counts[cell], uint32_t(__popc(peers)));
+        base = __shfl_sync(act, base, leader);
+        off[i] = base + uint32_t(__popc(peers & lanemask_lt()));
+    }
+}
+
+// ---- single-pass exclusive scan (decoupled look-back) -----------------------
+//
+// Tile = 256 threads x 16 items.  Warp w owns items [w*512, w*512+512) of the
+// tile as four 128-item chunks; lane l of chunk k holds items k*128 + 4l ..
+// k*128 + 4l + 3, so every load/store instruction is a fully coalesced 512-B
+// access.  The tile descriptor is one 64-bit word:
+//   [63:33] epoch tag (1..2^31-1), [32] 1 = inclusive prefix / 0 = aggregate,
+//   [31:0]  value (mod 2^32).
+// Tiles take their index from a monotonic ticket, so predecessors are always
+// resident or finished (no deadlock) and the epoch = ticket / tiles tells a
+// current descriptor from a stale one without clearing the array.
+
+__device__ __forceinline__ unsigned long long pack_status(uint32_t tag, uint32_t prefix,
+                                                          uint32_t v) {
+    return (static_cast<unsigned long long>(tag) << 33) |
+           (static_cast<unsigned long long>(prefix) << 32) | v;
+}
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+template <bool VEC>
+__device__ __forceinline__ void load4(const uint32_t* in, uint32_t idx, uint32_t n, uint32_t v[4]) {
+    if (VEC && idx + 3 < n) {
+        const uint4 q = *reinterpret_cast<const uint4*>(in + idx);
+        v[0] = q.x;
+        v[1] = q.y;
+        v[2] = q.z;
+        v[3] = q.w;
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) v[e] = (idx + e < n) ? in[idx + e] : 0u;
+    }
+}
+
+template <bool VEC>
+__device__ __forceinline__ void store4(uint32_t* out, uint32_t idx, uint32_t n, const uint32_t v[4]) {
+    if (VEC && idx + 3 < n) {
+        *reinterpret_cast<uint4*>(out + idx) = make_uint4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (idx + e < n) out[idx + e] = v[e];
+    }
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kScanThreads)
+k_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status,
+       unsigned long long* ticket, uint32_t tiles, int zero_input, uint32_t* err) {
+    __shared__ uint32_t s_tile, s_tag, s_warp[kScanThreads / 32], s_excl;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        const unsigned long long t = atomicAdd(ticket, 1ull);
+        s_tile = uint32_t(t % tiles);
+        s_tag = uint32_t((t / tiles) % 0x7fffffffull) + 1u;
+    }
+    __syncthreads();
+    const uint32_t tile = s_tile, tag = s_tag;
+    const uint32_t wbase = tile * kScanTile + warp * 512u;
+
+    uint32_t v[4][4], pre[4];
+    uint32_t running = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t idx = wbase + k * 128u + lane * 4u;
+        load4<VEC>(in, idx, n, v[k]);
+        const uint32_t t = v[k][0] + v[k][1] + v[k][2] + v[k][3];
+        uint32_t incl = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= uint32_t(o)) incl += y;
+        }
+        pre[k] = running + incl - t;
+        running += __shfl_sync(kFull, incl, 31);
+    }
+    if (zero_input) {
+        const uint32_t z[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) store4<VEC>(const_cast<uint32_t*>(in), wbase + k * 128u + lane * 4u, n, z);
+    }
+    if (lane == 0) s_warp[warp] = running;
+    __syncthreads();
+
+    if (warp == 0) {
+        // Block-level scan of the 8 warp totals.
+        const uint32_t wt = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+        uint32_t wincl = wt;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, wincl, o);
+            if (lane >= uint32_t(o)) wincl += y;
+        }
+        const uint32_t agg = __shfl_sync(kFull, wincl, kScanThreads / 32 - 1);
+        if (lane < kScanThreads / 32) s_warp[lane] = wincl - wt;
+
+        uint32_t excl = 0;
+        if (tile == 0) {
+            if (lane == 0) *(volatile unsigned long long*)&status[0] = pack_status(tag, 1u, agg);
+        } else {
+            if (lane == 0) *(volatile unsigned long long*)&status[tile] = pack_status(tag, 0u, agg);
+            int base = int(tile) - 1;
+            uint32_t spins = 0;
+            while (true) {
+                const int idx = base - int(lane);
+                const unsigned long long w =
+                    idx >= 0 ? *(volatile unsigned long long*)&status[idx] : pack_status(tag, 1u, 0u);
+                const bool valid = uint32_t(w >> 33) == tag;
+                if (__all_sync(kFull, valid)) {
+                    const unsigned pm = __ballot_sync(kFull, ((w >> 32) & 1ull) != 0ull);
+                    uint32_t val = uint32_t(w);
+                    if (pm) {
+                        const int first = __ffs(pm) - 1;
+                        if (int(lane) > first) val = 0;
+                        excl += warp_sum(val);
+                        break;
+                    }
+                    excl += warp_sum(val);
+                    base -= 32;
+                } else {
+                    if (++spins > kSpinLimit) {
+                        if (lane == 0) atomicOr(err, kDevErrSpin);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            if (lane == 0) *(volatile unsigned long long*)&status[tile] = pack_status(tag, 1u, excl + agg);
+        }
+        if (lane == 0) s_excl = excl;
+    }
+    __syncthreads();
+
+    const uint32_t tile_excl = s_excl + s_warp[warp];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint32_t o[4];
+        uint32_t r = tile_excl + pre[k];
+        o[0] = r;
+        r += v[k][0];
+        o[1] = r;
+        r += v[k][1];
+        o[2] = r;
+        r += v[k][2];
+        o[3] = r;
+        store4<VEC>(out, wbase + k * 128u + lane * 4u, n, o);
+    }
+}
+
+// scatterParticles (Spatial.metal:169-180) without the second atomic: the
+// rank came from the counting pass.
+__global__ void __launch_bounds__(256)
+k_scatter(uint32_t n, const uint32_t* __restrict__ hash, const uint32_t* __restrict__ off,
+          const uint32_t* __restrict__ cstart, uint32_t* __restrict__ tmp) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    tmp[cstart[hash[i]] + off[i]] = i;
+}
+
+// Stable re-rank inside the cell segment + gatherPositions (Spatial.metal:
+// 190-198).  Segments longer than kSegMax are queued for k_long_segments.
+__global__ void __launch_bounds__(256)
+k_sort_gather(uint32_t n, const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ hash,
+              const uint32_t* __restrict__ cstart, const float4* __restrict__ pos,
+              uint32_t* __restrict__ sidx, float4* __restrict__ sorted,
+              uint32_t* __restrict__ long_list, uint32_t* __restrict__ long_count) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t j = tmp[s];
+    const uint32_t c = hash[j];
+    const uint32_t a = cstart[c], b = cstart[c + 1];
+    if (b - a > kSegMax) {
+        if (s == a) long_list[atomicAdd(long_count, 1u)] = c;
+        return;
+    }
+    uint32_t rank = 0;
+    for (uint32_t k = a; k < b; ++k) rank += (tmp[k] < j) ? 1u : 0u;
+    const uint32_t d = a + rank;
+    sidx[d] = j;
+    sorted[d] = pos[j];
+}
+
+// Long segments: rank(j) = number of particles j' < j in the same cell, from
+// a block-wide scan over all particle indices.  One block per queued cell.
+__global__ void __launch_bounds__(256)
+k_long_segments(uint32_t n, const uint32_t* __restrict__ hash, const uint32_t* __restrict__ cstart,
+                const float4* __restrict__ pos, uint32_t* __restrict__ sidx,
+                float4* __restrict__ sorted, const uint32_t* __restrict__ long_list,
+                const uint32_t* __restrict__ long_count) {
+    __shared__ uint32_t s_warp[8];
+    const uint32_t total = *long_count;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t li = blockIdx.x; li < total; li += gridDim.x) {
+        const uint32_t c = long_list[li];
+        const uint32_t a = cstart[c], len = cstart[c + 1] - a;
+        uint32_t running = 0;
+        for (uint32_t base = 0; base < n && running < len; base += blockDim.x) {
+            const uint32_t j = base + threadIdx.x;
+            const bool f = j < n && hash[j] == c;
+            const unsigned m = __ballot_sync(kFull, f);
+            if (lane == 0) s_warp[warp] = __popc(m);
+            __syncthreads();
+            uint32_t before = 0, blk = 0;
+            for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+                if (w < warp) before += s_warp[w];
+                blk += s_warp[w];
+            }
+            if (f) {
+                const uint32_t d = a + running + before + __popc(m & lanemask_lt());
+                sidx[d] = j;
+                sorted[d] = pos[j];
+            }
+            running += blk;
+            __syncthreads();
+        }
+    }
+}
+
+// countNeighbors (Spatial.metal:207-243) in sorted order: the 27-cell
+// stencil is 9 contiguous slot ranges (x-fastest hash).
+__global__ void __launch_bounds__(256)
+k_count_neighbors(StepConsts c, const float4* __restrict__ sorted,
+                  const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ sidx,
+                  uint32_t* __restrict__ ncount) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= c.n) return;
+    const float4 p = sorted[s];
+    int cx, cy, cz;
+    cell_of(c.g, p.x, p.y, p.z, cx, cy, cz);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, c.g.gx - 1);
+    const int y0 = max(cy - 1, 0), y1 = min(cy + 1, c.g.gy - 1);
+    const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
+    uint32_t cnt = 0;
+    for (int z = z0; z <= z1; ++z)
+        for (int y = y0; y <= y1; ++y) {
+            const uint32_t a = cstart[cell_hash(c.g, x0, y, z)];
+            const uint32_t b = cstart[cell_hash(c.g, x1, y, z) + 1];
+            for (uint32_t k = a; k < b; ++k) {
+                const float4 q = __ldg(&sorted[k]);
+                const float r2 = dist2(q.x - p.x, q.y - p.y, q.z - p.z);
+                cnt += (r2 < c.h2) ? 1u : 0u;
+            }
+        }
+    ncount[sidx[s]] = cnt - 1u;  // the particle itself is in range (r = 0)
+}
+
+inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+cudaError_t launch_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status,
+                        unsigned long long* ticket, uint32_t tiles, bool zero_input, uint32_t* err,
+                        cudaStream_t s, KernelTimer* t) {
+    if (n == 0) return cudaSuccess;
+    const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0;
+    tbegin(t, s);
+    if (vec)
+        k_scan<true><<<tiles, kScanThreads, 0, s>>>(in, out, n, status, ticket, tiles, zero_input, err);
+    else
+        k_scan<false><<<tiles, kScanThreads, 0, s>>>(in, out, n, status, ticket, tiles, zero_input, err);
+    tend(t, "scan", s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hash_pass(const StepConsts& c, const DevState& d, bool predict, cudaStream_t s,
+                             KernelTimer* t) {
+    const uint32_t n = c.n;
+    tbegin(t, s);
+    k_predict_hash<<<n ? cdiv(n, 256) : 1, 256, 0, s>>>(c, d.pos, d.vel, d.prev, d.hash, d.off,
+                                                        d.counts, d.long_count, d.sphere,
+                                                        predict ? 1 : 0);
+    tend(t, predict ? "predict_hash" : "hash", s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = launch_scan(d.counts, d.cstart, c.g.cells + 1, d.scan_status, d.scan_ticket, d.scan_tiles,
+                    true, d.err, s, t);
+    if (e != cudaSuccess || n == 0) return e;
+    tbegin(t, s);
+    k_scatter<<<cdiv(n, 256), 256, 0, s>>>(n, d.hash, d.off, d.cstart, d.tmp);
+    tend(t, "scatter", s);
+    tbegin(t, s);
+    k_sort_gather<<<cdiv(n, 256), 256, 0, s>>>(n, d.tmp, d.hash, d.cstart, d.pos, d.sidx,
+                                                d.sorted_a, d.long_list, d.long_count);
+    tend(t, "sort_gather", s);
+    tbegin(t, s);
+    k_long_segments<<<148, 256, 0, s>>>(n, d.hash, d.cstart, d.pos, d.sidx, d.sorted_a,
+                                        d.long_list, d.long_count);
+    tend(t, "long_segments", s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_neighbors(const StepConsts& c, const DevState& d, cudaStream_t s,
+                                   KernelTimer* t) {
+    if (c.n == 0) return cudaSuccess;
+    tbegin(t, s);
+    k_count_neighbors<<<cdiv(c.n, 256), 256, 0, s>>>(c, d.sorted_a, d.cstart, d.sidx, d.ncount);
+    tend(t, "count_neighbors", s);
+    return cudaGetLastError();
+}
+
+}  // namespace mpb

@@ -1,0 +1,82 @@
+// pbf_kernels.h — host-side launchers of the PBF step kernels (sm_100a).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pbf_device.cuh"
+
+namespace mpb {
+
+// Device buffers of one scene (all sized for n particles / cells+1 cells).
+struct DevState {
+    float4* pos;            // positions, original order (predicted during a step)
+    float4* vel;            // velocities
+    float4* prev;           // positions at the start of the step
+    float4* sorted_a;       // sorted positions: hash-time gather, solver iterate
+    float4* sorted_b;       // sorted (position, lambda) written by the lambda pass
+    uint32_t* hash;         // cell hash per particle
+    uint32_t* off;          // rank of the particle's atomic increment in its cell
+    uint32_t* tmp;          // unstable cell-grouped order (before the stable fix-up)
+    uint32_t* sidx;         // sortedIndex: slot -> particle, stable within a cell
+    uint32_t* ncount;       // neighbour count per particle
+    float* lambdas;         // last lambda per particle
+    float* foam;            // foam intensity per particle
+    uint32_t* counts;       // cells+1 per-cell counts (all zero between passes)
+    uint32_t* cstart;       // cells+1 exclusive scan of counts
+    uint32_t* long_list;    // cells whose segment exceeds kSegMax
+    uint32_t* long_count;   // entries in long_list
+    unsigned long long* scan_status;  // look-back tile descriptors
+    unsigned long long* scan_ticket;  // monotonic tile ticket
+    uint32_t scan_tiles;
+    uint32_t* err;          // device error word (kDevErr*)
+    SphereState* sphere;    // sphere state (scene 2)
+};
+
+constexpr uint32_t kScanThreads = 256;
+constexpr uint32_t kScanItemsPerThread = 16;
+constexpr uint32_t kScanTile = kScanThreads * kScanItemsPerThread;  // 4096
+constexpr uint32_t kSegMax = 256;  // longest cell segment ranked in place
+
+inline uint32_t scan_tiles_for(uint64_t n) { return uint32_t((n + kScanTile - 1) / kScanTile); }
+
+// Optional per-kernel timing: the launchers call begin() before and end()
+// after every kernel they enqueue (CUDA events on the same stream).
+struct KernelTimer {
+    virtual void begin(cudaStream_t s) = 0;
+    virtual void end(const char* kernel, cudaStream_t s) = 0;
+    virtual ~KernelTimer() = default;
+};
+
+// Exclusive scan with decoupled look-back.  `status` holds `tiles` words and
+// `ticket` one word, both from an earlier call with the same tile count or
+// zeroed.  zero_input: write 0 over `in` after reading it.
+cudaError_t launch_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status,
+                        unsigned long long* ticket, uint32_t tiles, bool zero_input, uint32_t* err,
+                        cudaStream_t s, KernelTimer* t = nullptr);
+
+// Timer helpers for the launchers.
+inline void tbegin(KernelTimer* t, cudaStream_t s) {
+    if (t) t->begin(s);
+}
+inline void tend(KernelTimer* t, const char* k, cudaStream_t s) {
+    if (t) t->end(k, s);
+}
+
+// Spatial hash of the current (predict = false) or predicted (predict =
+// true) positions: fills hash, cstart, sidx, sorted_a (and counts back to
+// zero).  With predict, the sphere (if any) is advanced first.
+cudaError_t launch_hash_pass(const StepConsts& c, const DevState& d, bool predict, cudaStream_t s,
+                             KernelTimer* t = nullptr);
+// countNeighbors on sorted_a (buildSpatialHash only; the step fuses it).
+cudaError_t launch_count_neighbors(const StepConsts& c, const DevState& d, cudaStream_t s,
+                                   KernelTimer* t = nullptr);
+// K solver iterations + scatter-back + finalize + foam.
+cudaError_t launch_solver(const StepConsts& c, const DevState& d, uint32_t iterations,
+                          cudaStream_t s, KernelTimer* t = nullptr);
+
+// Number of kernel launches one step issues (for the benchmark's count).
+uint32_t step_launch_count(uint32_t iterations);
+
+}  // namespace mpb

@@ -1,0 +1,88 @@
+"""Tolerances and comparison helpers shared by the parity tests.
+
+Positions: within 1e-5 * h of the FP64 oracle per step, from the same FP32
+input state (the acceptance bound of the step).  Velocities are
+(p - p_prev) / dt * damping, so their bound is the position bound / dt.
+Integer outputs (cell hashes, cell starts, sorted order, neighbour counts)
+are compared bit for bit.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+H = 0.1
+POS_TOL = 1e-5 * H
+LAMBDA_ATOL = 2e-7
+LAMBDA_RTOL = 1e-4
+FOAM_ATOL = 1e-3
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_shaders.npz")
+
+
+def golden() -> dict:
+    z = np.load(GOLDEN)
+    return {k: z[k] for k in z.files}
+
+
+def max_abs(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max()) if a.size else 0.0
+
+
+def assert_positions(got, want, tol: float = POS_TOL, what: str = "positions") -> float:
+    err = max_abs(np.asarray(got)[:, :3], np.asarray(want)[:, :3])
+    assert err <= tol, f"{what}: max |diff| {err:.3e} > {tol:.3e}"
+    return err
+
+
+def assert_velocities(got, want, dt: float, tol: float = POS_TOL, what: str = "velocities") -> float:
+    bound = tol / dt
+    err = max_abs(np.asarray(got)[:, :3], np.asarray(want)[:, :3])
+    assert err <= bound, f"{what}: max |diff| {err:.3e} > {bound:.3e}"
+    return err
+
+
+def assert_lambdas(got, want) -> None:
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    bound = LAMBDA_ATOL + LAMBDA_RTOL * np.abs(want)
+    bad = np.abs(got - want) > bound
+    assert not bad.any(), f"lambda: {bad.sum()} outside tolerance, worst {np.abs(got - want).max():.3e}"
+
+
+def assert_equal_u32(got, want, what: str) -> None:
+    got = np.asarray(got)
+    want = np.asarray(want)
+    assert got.shape == want.shape, f"{what}: shape {got.shape} != {want.shape}"
+    if not np.array_equal(got, want):
+        i = int(np.nonzero(got != want)[0][0])
+        raise AssertionError(f"{what}: first mismatch at {i}: got {got[i]} want {want[i]}")
+
+
+def sensitivity(p, dt: float, pos4, vel4, sphere=None, seed: int = 0) -> float:
+    """How far the FP64 oracle's step moves when every input coordinate is
+    nudged by one FP32 ulp: the conditioning of the step at this state.  A
+    deep first contact with the sphere amplifies it by ~10^4 in the
+    reference algorithm itself (FP32 and FP64 alike)."""
+    from oracle import oracle as O
+
+    pos4 = np.asarray(pos4, np.float32)
+    rng = np.random.default_rng(seed)
+    pert = pos4.copy()
+    sgn = np.where(rng.random(pert[:, :3].shape) < 0.5, -np.inf, np.inf).astype(np.float32)
+    pert[:, :3] = np.nextafter(pert[:, :3], sgn)
+    s0 = None if sphere is None else np.array(sphere, np.float64)
+    s1 = None if sphere is None else np.array(sphere, np.float64)
+    a = O.step(p, dt, pos4, vel4, s0)["pos"]
+    b = O.step(p, dt, pert, vel4, s1)["pos"]
+    return max_abs(a, b)
+
+
+def position_tolerance(p, dt: float, pos4, vel4, sphere=None) -> float:
+    """1e-5 h where the step is well conditioned (a 1-ulp input change moves
+    it by less than that); otherwise 4x the measured sensitivity."""
+    kappa = sensitivity(p, dt, pos4, vel4, sphere)
+    return POS_TOL if kappa <= POS_TOL else 4.0 * kappa

@@ -1,0 +1,245 @@
+"""Engine::step on the GPU (engine/src/Engine.cpp:685-811) through the C ABI,
+against the reference's known answers (tests/test_pbf.cpp), the golden
+vectors of its shaders, and the FP64 oracle per step from the same FP32
+state: positions within 1e-5 h, integer outputs bit-exact."""
+import numpy as np
+import pytest
+
+from mtlphys_b200 import Engine, _abi, configs
+from oracle import oracle as O
+from parity import (POS_TOL, assert_equal_u32, assert_lambdas, assert_positions,
+                    assert_velocities, golden, position_tolerance)
+
+pytestmark = pytest.mark.gpu
+G = golden()
+
+
+@pytest.fixture(scope="module")
+def eng(cuda):
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+def load_state(e, pos, vel, params=None, scene=_abi.MP_SCENE_CUBE_DROP):
+    if params is not None:
+        e.set_params(params)
+    e.reset(len(pos), scene)
+    e.set_positions(pos)
+    e.set_velocities(vel)
+
+
+def gpu_step(e, dt):
+    e.step(dt)
+    assert e.check_errors() == 0
+    return {"pos": e.positions(), "vel": e.velocities(), "lambda": e.lambdas(),
+            "neighbor_counts": e.neighbor_counts(), "foam": e.foam(), "hashes": e.cell_hashes(),
+            "sorted_index": e.sorted_index(), "cell_start": e.cell_start()}
+
+
+def compare_with_oracle(p, dt, pos, vel, got, sphere=None, check_lambda=True):
+    tol = position_tolerance(p, dt, pos, vel, sphere)
+    o = O.step(p, dt, pos, vel, None if sphere is None else np.array(sphere, np.float64))
+    assert_equal_u32(got["hashes"], o["hashes"], "hashes")
+    assert_equal_u32(got["cell_start"], o["cell_start"], "cellStart")
+    assert_equal_u32(got["sorted_index"], o["sorted_index"], "sortedIndex")
+    assert_equal_u32(got["neighbor_counts"], o["neighbor_counts"], "neighbor counts")
+    err = assert_positions(got["pos"], o["pos"], tol)
+    assert_velocities(got["vel"], o["vel"], dt, tol)
+    if check_lambda and tol == POS_TOL:
+        assert_lambdas(got["lambda"], o["lambda"])
+        assert np.abs(got["foam"] - o["foam"]).max() < 1e-3
+    assert (got["pos"][:, 3] == 1.0).all() and (got["vel"][:, 3] == 0.0).all()
+    return err
+
+
+# ---- tests/test_pbf.cpp ------------------------------------------------------------
+
+def test_isolated_particle_falls(eng):
+    load_state(eng, np.array([[0, 1, 0, 1]], np.float32), np.zeros((1, 4), np.float32),
+               _abi.default_params())
+    g = gpu_step(eng, 0.01)
+    assert g["pos"][0, 1] == pytest.approx(0.99902, rel=1e-3)
+    assert g["vel"][0, 1] < 0
+    assert_positions(g["pos"], G["pbf/isolated/pos"])
+
+
+def test_lambda_sign_and_isolated_value(eng):
+    p = _abi.default_params()
+    pos = G["pbf/lambda/pos_in"]
+    load_state(eng, pos, np.zeros_like(pos), p)
+    g = gpu_step(eng, 1e-6)
+    lam = g["lambda"]
+    assert lam[13] < 0
+    h = np.float64(np.float32(0.1))
+    w0 = 315.0 / (64.0 * np.pi * h ** 9) * h ** 6
+    assert lam[-1] == pytest.approx(-(w0 / p.rest_density - 1.0) / p.epsilon, rel=1e-5)
+    assert_lambdas(lam, G["pbf/lambda/lambda"])
+
+
+def test_fifty_steps_stay_finite_and_in_box(eng):
+    eng.set_params(_abi.default_params())
+    eng.reset(1024, _abi.MP_SCENE_CUBE_DROP)
+    for _ in range(50):
+        eng.step(1.0 / 240.0)
+    assert eng.check_errors() == 0
+    pos = eng.positions()
+    assert np.isfinite(pos).all()
+    assert (pos[:, 0] >= -3.01).all() and (pos[:, 0] <= 3.01).all()
+    assert (pos[:, 1] >= -3.01).all() and (pos[:, 1] <= 6.01).all()
+
+
+TRAJ = sorted({k.rsplit("/", 2)[0] + "/" + k.rsplit("/", 2)[1] for k in G if k.startswith("traj/")})
+
+
+@pytest.mark.parametrize("key", TRAJ)
+def test_step_matches_reference_shaders(eng, key):
+    k = key + "/"
+    p = _abi.default_params()
+    dt = float(G[k + "dt"])
+    sphere = G.get(k + "sphere_in")
+    scene = _abi.MP_SCENE_SPHERE_DROP if sphere is not None else _abi.MP_SCENE_CUBE_DROP
+    load_state(eng, G[k + "pos_in"], G[k + "vel_in"], p, scene)
+    if sphere is not None:
+        eng.set_sphere(sphere[:3], sphere[3:6], sphere[6])
+    g = gpu_step(eng, dt)
+    tol = position_tolerance(p, dt, G[k + "pos_in"], G[k + "vel_in"], sphere)
+    assert_equal_u32(g["hashes"], G[k + "hashes"], "hashes")
+    assert_equal_u32(g["sorted_index"], G[k + "sorted_index"], "sortedIndex")
+    assert_equal_u32(g["neighbor_counts"], G[k + "neighbor_counts"], "neighbor counts")
+    assert_positions(g["pos"], G[k + "pos"], max(tol, 2 * POS_TOL) if tol > POS_TOL else tol)
+    if sphere is not None:
+        s = eng.sphere()
+        assert np.abs(s[:6] - G[k + "sphere_out"][:6]).max() < 1e-5
+    compare_with_oracle(p, dt, G[k + "pos_in"], G[k + "vel_in"], g, sphere)
+
+
+# ---- the benchmark workloads, per step against the FP64 oracle ------------------------
+
+def run_and_check(e, w, check_at, steps, seed_check=True):
+    e.set_params(w.params)
+    e.reset(w.n, w.scene, w.desc)
+    pos = e.positions()
+    if seed_check:
+        want = O.seed_scene(w.params, w.scene, w.n, w.desc)
+        assert np.array_equal(pos, want), "seeded lattice differs from the oracle's"
+    errs = []
+    for st in range(steps):
+        if st in check_at:
+            pos, vel = e.positions(), e.velocities()
+            sphere = e.sphere() if w.scene == _abi.MP_SCENE_SPHERE_DROP else None
+            g = gpu_step(e, w.dt)
+            errs.append(compare_with_oracle(w.params, w.dt, pos, vel, g, sphere))
+        else:
+            e.step(w.dt)
+    assert e.check_errors() == 0
+    return errs
+
+
+def test_cube_drop_97k_per_step_parity(eng):
+    errs = run_and_check(eng, configs.cube_drop(), {0, 25, 79}, 80)
+    print("cube_drop max |dpos|:", errs)
+
+
+def test_dam_break_1m_per_step_parity(eng):
+    errs = run_and_check(eng, configs.dam_break(), {0, 12}, 13)
+    print("dam_break max |dpos|:", errs)
+
+
+def test_reference_sphere_drop_scene(eng):
+    eng.set_params(_abi.default_params())
+    eng.reset(30_000, _abi.MP_SCENE_SPHERE_DROP)
+    s = eng.sphere()
+    assert s[1] == pytest.approx(4.5) and s[6] == pytest.approx(0.6)
+    for st in range(3):
+        pos, vel, sph = eng.positions(), eng.velocities(), eng.sphere()
+        g = gpu_step(eng, 1.0 / 120.0)
+        compare_with_oracle(_abi.default_params(), 1.0 / 120.0, pos, vel, g, sph)
+
+
+def test_zero_iterations(eng):
+    p = _abi.default_params()
+    p.solver_iterations = 0
+    eng.set_params(p)
+    eng.reset(5000, _abi.MP_SCENE_DAM_BREAK)
+    pos, vel = eng.positions(), eng.velocities()
+    g = gpu_step(eng, 1.0 / 240.0)
+    compare_with_oracle(p, 1.0 / 240.0, pos, vel, g, check_lambda=False)
+
+
+def test_graph_mode_is_bit_identical(eng):
+    w = configs.cube_drop(side=30)
+    outs = []
+    for graph in (False, True):
+        eng.set_params(w.params)
+        eng.reset(w.n, w.scene, w.desc)
+        eng.set_graph_mode(graph)
+        for _ in range(20):
+            eng.step(w.dt)
+        assert eng.check_errors() == 0
+        outs.append((eng.positions(), eng.velocities(), eng.foam()))
+        eng.set_graph_mode(False)
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
+def test_steps_are_deterministic(eng):
+    w = configs.cube_drop(side=24)
+    outs = []
+    for _ in range(2):
+        eng.set_params(w.params)
+        eng.reset(w.n, w.scene, w.desc)
+        for _ in range(15):
+            eng.step(w.dt)
+        outs.append(eng.positions())
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_dt_le_zero_is_a_noop(eng):
+    eng.set_params(_abi.default_params())
+    eng.reset(1000)
+    before = eng.positions()
+    eng.step(0.0)
+    eng.step(-1.0)
+    assert np.array_equal(before, eng.positions())
+
+
+def test_nan_input_sets_the_device_error_word(eng):
+    eng.set_params(_abi.default_params())
+    eng.reset(1000)
+    pos = eng.positions()
+    pos[17, 0] = np.nan
+    eng.set_positions(pos)
+    eng.step(1.0 / 240.0)
+    bits = eng.error_bits()
+    assert bits & _abi.MP_DEVERR_NAN
+    assert eng.error_bits() == 0  # cleared
+
+
+def test_empty_engine_steps(eng):
+    eng.set_params(_abi.default_params())
+    eng.reset(0)
+    eng.step(1.0 / 240.0)
+    eng.build_spatial_hash()
+    assert eng.check_errors() == 0
+    assert eng.particle_count() == 0
+
+
+def with_reference_k(w):
+    """The same workload with the reference engine's s_corr k = 1e-4
+    (Constraints.metal:158), where the step is well conditioned."""
+    w.params = w.params.copy()
+    w.params.scorr_k = 1e-4
+    return w
+
+
+def test_cube_drop_97k_reference_k_strict_parity(eng):
+    errs = run_and_check(eng, with_reference_k(configs.cube_drop()), {0, 40, 99}, 100)
+    assert max(errs) <= POS_TOL
+    print("cube_drop (k=1e-4) max |dpos|:", errs)
+
+
+def test_dam_break_1m_reference_k_strict_parity(eng):
+    errs = run_and_check(eng, with_reference_k(configs.dam_break()), {0, 20}, 21)
+    assert max(errs) <= POS_TOL
+    print("dam_break (k=1e-4) max |dpos|:", errs)
