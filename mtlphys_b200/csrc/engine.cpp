@@ -87,6 +87,7 @@ int make_grid(const mp_pbf_params& p, GridDev& g) {
     g.oy = p.bounds_min[1];
     g.oz = p.bounds_min[2];
     g.inv = 1.0f / p.cell_size;
+    g.cs = p.cell_size;
     g.gx = int(dims[0]);
     g.gy = int(dims[1]);
     g.gz = int(dims[2]);
@@ -364,7 +365,7 @@ struct mp_engine {
         free_particles();
         const size_t v4 = size_t(cap) * 16, u = size_t(cap) * 4;
         const size_t longs = (size_t(cap) / mpb::kSegMax + 2) * 4;
-        const size_t total = 5 * v4 + 7 * u + longs + 256;
+        const size_t total = 5 * v4 + 8 * u + longs + 16 * 256;
         MP_CUDA(cudaMalloc(&particle_block, total));
         char* b = static_cast<char*>(particle_block);
         auto take = [&](size_t bytes) {
@@ -381,6 +382,7 @@ struct mp_engine {
         d.off = reinterpret_cast<uint32_t*>(take(u));
         d.tmp = reinterpret_cast<uint32_t*>(take(u));
         d.sidx = reinterpret_cast<uint32_t*>(take(u));
+        d.scell = reinterpret_cast<uint32_t*>(take(u));
         d.ncount = reinterpret_cast<uint32_t*>(take(u));
         d.lambdas = reinterpret_cast<float*>(take(u));
         d.foam = reinterpret_cast<float*>(take(u));
@@ -455,6 +457,7 @@ struct mp_engine {
         c.inv_dt = 1.0f / dt;
         c.damping = p.damping;
         c.vmax = p.vmax * h * c.inv_dt;
+        c.vmax_frac = p.vmax;
         c.wall_eps = p.wall_eps;
         c.floor_fric = p.floor_friction;
         c.wall_fric = p.wall_friction;

@@ -21,6 +21,7 @@ namespace mpb {
 struct GridDev {
     float ox, oy, oz;  // gridOrigin (= bounds_min)
     float inv;         // invCellSize = 1.0f / cellSize, rounded on the host
+    float cs;          // cellSize
     int gx, gy, gz;    // gridDim
     uint32_t cells;    // gx * gy * gz
 };
@@ -36,7 +37,7 @@ struct StepConsts {
     uint32_t scorr_n;
     float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
     float gravx, gravy, gravz;
-    float dt, inv_dt, damping, vmax;
+    float dt, inv_dt, damping, vmax, vmax_frac;
     float wall_eps, floor_fric, wall_fric;
     float foam_maxn, foam_lo, foam_hi;
     int sphere;  // 1: sphere-drop scene (sphere state lives in device memory)

@@ -353,7 +353,9 @@ k_count_neighbors(StepConsts c, const float4* __restrict__ sorted,
                 cnt += (r2 < c.h2) ? 1u : 0u;
             }
         }
-    ncount[sidx[s]] = cnt - 1u;  // the particle itself is in range (r = 0)
+    // the particle itself passed its own distance test unless its position is
+    // not finite
+    ncount[sidx[s]] = cnt - (dist2(p.x - p.x, p.y - p.y, p.z - p.z) < c.h2 ? 1u : 0u);
 }
 
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }

@@ -20,6 +20,7 @@ struct DevState {
     uint32_t* off;          // rank of the particle's atomic increment in its cell
     uint32_t* tmp;          // unstable cell-grouped order (before the stable fix-up)
     uint32_t* sidx;         // sortedIndex: slot -> particle, stable within a cell
+    uint32_t* scell;        // hash cell per sorted slot (anchor of the solver state)
     uint32_t* ncount;       // neighbour count per particle
     float* lambdas;         // last lambda per particle
     float* foam;            // foam intensity per particle

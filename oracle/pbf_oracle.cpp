@@ -183,11 +183,18 @@ void sphere_advance(const Consts& c, double dt, double* s) {
     }
 }
 
+// Metal's clamp(x, lo, hi) = fmin(fmax(x, lo), hi): a NaN coordinate goes to
+// the lower bound.
+inline double clampd(double x, double lo, double hi) { return std::fmin(std::fmax(x, lo), hi); }
+
 // The shared FP64 step.  `pos`/`vel` are the state at the start of the step
 // (FP64, original order), `pred32` the FP32 predicted positions the hash is
-// built on.  Writes every output that is non-NULL.
+// built on.  solve_from_pred32: the solver starts from those FP32 predicted
+// positions (the reference's own predict arithmetic, bit-exact with the
+// product) instead of the FP64 prediction.  Writes every non-NULL output.
 int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, const V3* vel,
-              const float* pred32, double* sphere, V3* pos_out, V3* vel_out, or_step_out* out) {
+              const float* pred32, bool solve_from_pred32, double* sphere, V3* pos_out,
+              V3* vel_out, or_step_out* out) {
     or_grid g;
     if (or_make_grid(p, &g) != 0) return MP_ERR_INVALID_ARGUMENT;
     const Consts c = make_consts(p, g, dt);
@@ -202,8 +209,12 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
     std::vector<V3> pred(n);
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < int64_t(n); ++i) {
-        const V3 vn = {vel[i].x + c.g[0] * dt, vel[i].y + c.g[1] * dt, vel[i].z + c.g[2] * dt};
-        pred[i] = pos[i] + dt * vn;
+        if (solve_from_pred32) {
+            pred[i] = {pred32[4 * i], pred32[4 * i + 1], pred32[4 * i + 2]};
+        } else {
+            const V3 vn = {vel[i].x + c.g[0] * dt, vel[i].y + c.g[1] * dt, vel[i].z + c.g[2] * dt};
+            pred[i] = pos[i] + dt * vn;
+        }
     }
 
     // 2. spatial hash on the FP32 predicted positions.
@@ -266,15 +277,15 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
             const double dl = std::sqrt(dot(d, d));
             if (dl > c.max_step) d = (c.max_step / dl) * d;
             V3 np = pi + d;
-            np.x = std::min(std::max(np.x, c.bmin[0]), c.bmax[0]);
-            np.y = std::min(std::max(np.y, c.bmin[1]), c.bmax[1]);
-            np.z = std::min(std::max(np.z, c.bmin[2]), c.bmax[2]);
+            np.x = clampd(np.x, c.bmin[0], c.bmax[0]);
+            np.y = clampd(np.y, c.bmin[1], c.bmax[1]);
+            np.z = clampd(np.z, c.bmin[2], c.bmax[2]);
             if (sphere) {
                 const V3 ctr = {sph[0], sph[1], sph[2]};
                 const V3 dd = np - ctr;
                 const double r2 = dot(dd, dd);
                 if (r2 < rr) {
-                    const double r = std::sqrt(std::max(r2, double(1e-8f)));
+                    const double r = std::sqrt(std::fmax(r2, double(1e-8f)));
                     np = ctr + (sph[6] / r) * dd;
                 }
             }
@@ -293,9 +304,9 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < int64_t(n); ++i) {
         V3 q = pfin[i];
-        q.x = std::min(std::max(q.x, c.bmin[0]), c.bmax[0]);
-        q.y = std::min(std::max(q.y, c.bmin[1]), c.bmax[1]);
-        q.z = std::min(std::max(q.z, c.bmin[2]), c.bmax[2]);
+        q.x = clampd(q.x, c.bmin[0], c.bmax[0]);
+        q.y = clampd(q.y, c.bmin[1], c.bmax[1]);
+        q.z = clampd(q.z, c.bmin[2], c.bmax[2]);
         V3 v = {(q.x - pos[i].x) * c.inv_dt * c.damping, (q.y - pos[i].y) * c.inv_dt * c.damping,
                 (q.z - pos[i].z) * c.inv_dt * c.damping};
         const bool xMin = q.x <= c.bmin[0] + c.wall_eps;
@@ -304,12 +315,12 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
         const bool yMax = q.y >= c.bmax[1] - c.wall_eps;
         const bool zMin = q.z <= c.bmin[2] + c.wall_eps;
         const bool zMax = q.z >= c.bmax[2] - c.wall_eps;
-        if (xMin) v.x = std::max(v.x, 0.0);
-        if (xMax) v.x = std::min(v.x, 0.0);
-        if (yMin) v.y = std::max(v.y, 0.0);
-        if (yMax) v.y = std::min(v.y, 0.0);
-        if (zMin) v.z = std::max(v.z, 0.0);
-        if (zMax) v.z = std::min(v.z, 0.0);
+        if (xMin) v.x = std::fmax(v.x, 0.0);
+        if (xMax) v.x = std::fmin(v.x, 0.0);
+        if (yMin) v.y = std::fmax(v.y, 0.0);
+        if (yMax) v.y = std::fmin(v.y, 0.0);
+        if (zMin) v.z = std::fmax(v.z, 0.0);
+        if (zMax) v.z = std::fmin(v.z, 0.0);
         if (yMin) {
             v.x *= c.floor_fric;
             v.z *= c.floor_fric;
@@ -321,7 +332,7 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
         pfin[i] = q;
         vfin[i] = v;
         const double surface =
-            1.0 - std::min(std::max(double(ncount[i]) / c.foam_maxn, 0.0), 1.0);
+            1.0 - clampd(double(ncount[i]) / c.foam_maxn, 0.0, 1.0);
         foam[i] = surface * smoothstep(c.foam_lo, c.foam_hi, std::sqrt(dot(v, v)));
     }
 
@@ -529,8 +540,8 @@ int or_step(const mp_pbf_params* p, float dt, uint32_t n, const float* pos4, con
     }
     std::vector<float> pred32(4 * size_t(n));
     or_predict_f32(pos4, vel4, n, p->gravity, dt, pred32.data());
-    return step_core(p, double(dt), n, pos.data(), vel.data(), pred32.data(), sphere, nullptr,
-                     nullptr, out);
+    return step_core(p, double(dt), n, pos.data(), vel.data(), pred32.data(), true, sphere,
+                     nullptr, nullptr, out);
 }
 
 int or_step_f64(const mp_pbf_params* p, double dt, uint32_t n, double* pos3, double* vel3,
@@ -545,7 +556,8 @@ int or_step_f64(const mp_pbf_params* p, double dt, uint32_t n, double* pos3, dou
     const V3* pos = reinterpret_cast<const V3*>(pos3);
     const V3* vel = reinterpret_cast<const V3*>(vel3);
     std::vector<V3> po(n), vo(n);
-    const int rc = step_core(p, dt, n, pos, vel, pred32.data(), sphere, po.data(), vo.data(), nullptr);
+    const int rc =
+        step_core(p, dt, n, pos, vel, pred32.data(), false, sphere, po.data(), vo.data(), nullptr);
     if (rc) return rc;
     std::memcpy(pos3, po.data(), sizeof(V3) * n);
     std::memcpy(vel3, vo.data(), sizeof(V3) * n);

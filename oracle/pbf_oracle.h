@@ -86,15 +86,16 @@ typedef struct or_step_out {
  * One Engine::step in FP64 from an FP32 particle state (float4 x n).
  *   sphere: NULL unless the scene is the sphere drop; advanced in place.
  * The hash is built on FP32 predicted positions (or_predict_f32) so that its
- * integer outputs match the CUDA path bit for bit; the solver starts from
- * the FP64 predicted positions.
+ * integer outputs match the CUDA path bit for bit, and the FP64 solver starts
+ * from those same FP32 predicted positions (the reference computes its
+ * prediction in FP32; everything after it is FP64 here).
  */
 int or_step(const mp_pbf_params* p, float dt, uint32_t n, const float* pos4, const float* vel4,
             double* sphere, or_step_out* out);
 
 /*
- * One step with an FP64 state (xyz triples) in and out: the hash is built on
- * the FP64 predicted positions rounded to FP32.  Used for FP64 rollouts
+ * One step with an FP64 state (xyz triples) in and out: the prediction is
+ * FP64 and the hash is built on it rounded to FP32.  Used for FP64 rollouts
  * (finite differences of the adjoint).  pos3/vel3 are updated in place.
  */
 int or_step_f64(const mp_pbf_params* p, double dt, uint32_t n, double* pos3, double* vel3,

@@ -8,7 +8,7 @@ import pytest
 from mtlphys_b200 import Engine, _abi, configs
 from oracle import oracle as O
 from parity import (POS_TOL, assert_equal_u32, assert_lambdas, assert_positions,
-                    assert_velocities, golden, position_tolerance)
+                    assert_velocities, golden, position_tolerance, sensitivity)
 
 pytestmark = pytest.mark.gpu
 G = golden()
@@ -40,6 +40,9 @@ def gpu_step(e, dt):
 def compare_with_oracle(p, dt, pos, vel, got, sphere=None, check_lambda=True):
     tol = position_tolerance(p, dt, pos, vel, sphere)
     o = O.step(p, dt, pos, vel, None if sphere is None else np.array(sphere, np.float64))
+    d = np.abs(got["pos"][:, :3] - o["pos"]).max(axis=1)
+    print(f"  n={len(pos)} max|dpos|={d.max():.3e} p99.9={np.percentile(d, 99.9):.3e} "
+          f"p50={np.median(d):.3e} tol={tol:.3e}")
     assert_equal_u32(got["hashes"], o["hashes"], "hashes")
     assert_equal_u32(got["cell_start"], o["cell_start"], "cellStart")
     assert_equal_u32(got["sorted_index"], o["sorted_index"], "sortedIndex")
@@ -107,7 +110,8 @@ def test_step_matches_reference_shaders(eng, key):
     assert_equal_u32(g["hashes"], G[k + "hashes"], "hashes")
     assert_equal_u32(g["sorted_index"], G[k + "sorted_index"], "sortedIndex")
     assert_equal_u32(g["neighbor_counts"], G[k + "neighbor_counts"], "neighbor counts")
-    assert_positions(g["pos"], G[k + "pos"], max(tol, 2 * POS_TOL) if tol > POS_TOL else tol)
+    # two FP32 implementations, each within the bound of the FP64 oracle
+    assert_positions(g["pos"], G[k + "pos"], 2 * tol)
     if sphere is not None:
         s = eng.sphere()
         assert np.abs(s[:6] - G[k + "sphere_out"][:6]).max() < 1e-5
