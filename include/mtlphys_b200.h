@@ -45,7 +45,7 @@ extern "C" {
 
 /* bits of the device error word (mp_engine_check_errors) */
 #define MP_DEVERR_SPIN_LIMIT     0x1u  /* scan look-back / grid barrier timed out */
-#define MP_DEVERR_NAN            0x2u  /* a non-finite position left a step       */
+#define MP_DEVERR_NAN            0x2u  /* a non-finite position or velocity entered or left a step */
 #define MP_DEVERR_INDEX          0x4u  /* an index check failed (debug checks)    */
 
 /* ---- scenes: Engine.hpp:37-39 ------------------------------------------- */

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256)
 k_predict_hash(StepConsts c, float4* __restrict__ pos, const float4* __restrict__ vel,
                float4* __restrict__ prev, uint32_t* __restrict__ hash, uint32_t* __restrict__ off,
                uint32_t* __restrict__ counts, uint32_t* __restrict__ long_count,
-               SphereState* __restrict__ sphere, int predict) {
+               SphereState* __restrict__ sphere, int predict, uint32_t* __restrict__ err) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *long_count = 0;
         if (predict && c.sphere) sphere_advance(c, sphere);
@@ -78,6 +78,9 @@ k_predict_hash(StepConsts c, float4* __restrict__ pos, const float4* __restrict_
         float4 p = pos[i];
         if (predict) {
             const float4 v = vel[i];
+            // A non-finite input survives as a finite clamped position (the
+            // reference's clamp semantics), so flag it here, on entry.
+            if (!isfinite(p.x + p.y + p.z + v.x + v.y + v.z)) atomicOr(err, kDevErrNaN);
             prev[i] = p;
             // v' = v + g*dt and p' = p + v'*dt, each one fused multiply-add.
             const float vx = __fmaf_rn(c.gravx, c.dt, v.x);
@@ -382,7 +385,7 @@ cudaError_t launch_hash_pass(const StepConsts& c, const DevState& d, bool predic
     tbegin(t, s);
     k_predict_hash<<<n ? cdiv(n, 256) : 1, 256, 0, s>>>(c, d.pos, d.vel, d.prev, d.hash, d.off,
                                                         d.counts, d.long_count, d.sphere,
-                                                        predict ? 1 : 0);
+                                                        predict ? 1 : 0, d.err);
     tend(t, predict ? "predict_hash" : "hash", s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

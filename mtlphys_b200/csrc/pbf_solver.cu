@@ -107,18 +107,23 @@ __device__ __forceinline__ void for_stencil_anchored(const StepConsts& c, const 
     const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
     const float aix = anchor(c.g.ox, c.g.cs, pcx), aiy = anchor(c.g.oy, c.g.cs, pcy),
                 aiz = anchor(c.g.oz, c.g.cs, pcz);
+    // the particle's x offset from the anchors of the (up to) three x cells
+    const int nx = x1 - x0 + 1;
+    const float ox0 = (aix - anchor(c.g.ox, c.g.cs, x0)) + lx;
+    const float ox1 = (aix - anchor(c.g.ox, c.g.cs, x0 + 1)) + lx;
+    const float ox2 = (aix - anchor(c.g.ox, c.g.cs, x0 + 2)) + lx;
     for (int z = z0; z <= z1; ++z) {
         const float oz = (aiz - anchor(c.g.oz, c.g.cs, z)) + lz;
         for (int y = y0; y <= y1; ++y) {
             const float oy = (aiy - anchor(c.g.oy, c.g.cs, y)) + ly;
-            const uint32_t row = cell_hash(c.g, 0, y, z);
-            uint32_t b = cstart[row + x0];
-            for (int x = x0; x <= x1; ++x) {
-                const uint32_t e = cstart[row + x + 1];
-                const float ox = (aix - anchor(c.g.ox, c.g.cs, x)) + lx;
-                for (uint32_t k = b; k < e; ++k) f(k, ox, oy, oz);
-                b = e;
-            }
+            // all cell boundaries of the row up front (independent loads)
+            const uint32_t base = cell_hash(c.g, x0, y, z);
+            const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
+            const uint32_t b2 = nx > 1 ? cstart[base + 2] : b1;
+            const uint32_t b3 = nx > 2 ? cstart[base + 3] : b2;
+            for (uint32_t k = b0; k < b1; ++k) f(k, ox0, oy, oz);
+            for (uint32_t k = b1; k < b2; ++k) f(k, ox1, oy, oz);
+            for (uint32_t k = b2; k < b3; ++k) f(k, ox2, oy, oz);
         }
     }
 }

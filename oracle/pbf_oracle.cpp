@@ -140,10 +140,13 @@ Consts make_consts(const mp_pbf_params* p, const or_grid& g, double dt) {
     return c;
 }
 
-inline void cell_coord_f64(const Consts& c, V3 p, int out[3]) {
-    const double v[3] = {p.x, p.y, p.z};
-    for (int a = 0; a < 3; ++a)
-        out[a] = clampi(floor_to_int_sat((v[a] - c.origin[a]) * c.inv_cell), 0, c.dims[a] - 1);
+// Stencil cell of the current iterate: the reference derives it from its
+// FP32 position with cellCoordOf (Constraints.metal:94, 152), so the FP64
+// iterate is rounded to FP32 and put through the same FP32 formula.  (A plain
+// FP64 floor would disagree with the reference exactly at cell faces, where
+// the stencil, and so the result, is discontinuous.)
+inline void cell_coord_iter(const or_grid& g, V3 p, int out[3]) {
+    cell_coord_f32(g, float(p.x), float(p.y), float(p.z), out);
 }
 
 // Visit the 27-cell stencil around `cc` as 9 contiguous slot ranges, in the
@@ -236,7 +239,7 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
         for (int64_t s = 0; s < int64_t(n); ++s) {
             const V3 pi = cur[s];
             int cc[3];
-            cell_coord_f64(c, pi, cc);
+            cell_coord_iter(g, pi, cc);
             double dens = poly6(0.0, c), gsq = 0.0;
             V3 gs = {0, 0, 0};
             for_stencil(g, cc, cell_start.data(), [&](uint32_t k) {
@@ -259,7 +262,7 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
             const V3 pi = cur[s];
             const double li = lam[s];
             int cc[3];
-            cell_coord_f64(c, pi, cc);
+            cell_coord_iter(g, pi, cc);
             V3 d = {0, 0, 0};
             for_stencil(g, cc, cell_start.data(), [&](uint32_t k) {
                 if (k == uint32_t(s)) return;
