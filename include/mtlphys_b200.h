@@ -218,6 +218,19 @@ size_t mp_exclusive_scan_scratch_bytes(uint32_t n);
 int mp_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n,
                       void* scratch, size_t scratch_bytes, mp_stream stream);
 
+/* The same exclusive scan without any device allocation, for callers that
+ * cannot allocate when they need it (a frame loop with a fixed per-frame
+ * memory budget, a host framework whose allocator owns the device heap).
+ * It has no counterpart in the reference.  Its scratch is a 33,024-byte
+ * static device array held by every GPU that loads this library, which
+ * limits n to 16,777,216 (2^24) elements: larger n returns
+ * MP_ERR_INVALID_ARGUMENT.  `in` and `out` are device pointers on the current
+ * device.  The first call on each device looks up the array's address (set-up
+ * with that device current); make that first call before any stream capture.
+ * All calls share the one array, so calls that overlap on the GPU (other
+ * streams, other host threads) race: order them on one stream. */
+int mp_exclusive_scan_noalloc(const uint32_t* in, uint32_t* out, uint32_t n, mp_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

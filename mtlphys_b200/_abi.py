@@ -160,6 +160,7 @@ PROTOTYPES = {
     "mp_engine_synchronize": (_INT, [_VP]),
     "mp_exclusive_scan_scratch_bytes": (_SZ, [_U32]),
     "mp_exclusive_scan": (_INT, [_VP, _VP, _U32, _VP, _SZ, _VP]),
+    "mp_exclusive_scan_noalloc": (_INT, [_VP, _VP, _U32, _VP]),
 }
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmtlphys_b200.so")

@@ -484,6 +484,14 @@ extern "C" {
 
 const char* mp_last_error(void) { return g_err.c_str(); }
 
+}  // extern "C"
+
+// Lets the other translation units of the library report through
+// mp_last_error().
+void mpb::record_error(const char* msg) { g_err = msg; }
+
+extern "C" {
+
 uint32_t mp_abi_version(void) { return kAbiVersion; }
 
 int mp_default_params(mp_pbf_params* out) {

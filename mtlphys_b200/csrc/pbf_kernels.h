@@ -80,4 +80,7 @@ cudaError_t launch_solver(const StepConsts& c, const DevState& d, uint32_t itera
 // Number of kernel launches one step issues (for the benchmark's count).
 uint32_t step_launch_count(uint32_t iterations);
 
+// Sets the message mp_last_error() returns on this thread.
+void record_error(const char* msg);
+
 }  // namespace mpb
