@@ -321,6 +321,7 @@ struct mp_engine {
     uint32_t n_alloc = 0;      // particle capacity of the buffers
     uint32_t cells_alloc = 0;  // grid cells the cell buffers were sized for (0: none)
     void* particle_block = nullptr;
+    void* list_block = nullptr;  // in-range row masks of the solver
     void* cell_block = nullptr;
     void* small_block = nullptr;
     mpb::SphereState sphere_init{};
@@ -341,7 +342,12 @@ struct mp_engine {
     }
     void free_particles() {
         if (particle_block) cudaFree(particle_block);
+        if (list_block) cudaFree(list_block);
         particle_block = nullptr;
+        list_block = nullptr;
+        d.row_masks = nullptr;
+        d.mask_overflow = nullptr;
+        d.mask_stride = 0;
         n_alloc = 0;
     }
     void free_cells() {
@@ -388,6 +394,11 @@ struct mp_engine {
         d.foam = reinterpret_cast<float*>(take(u));
         d.long_list = reinterpret_cast<uint32_t*>(take(longs));
         MP_CUDA(cudaMemset(particle_block, 0, total));
+        // 9 row masks (4 bytes each) + an overflow flag per particle
+        MP_CUDA(cudaMalloc(&list_block, 10 * u));
+        d.row_masks = static_cast<uint32_t*>(list_block);
+        d.mask_overflow = d.row_masks + 9 * size_t(cap);
+        d.mask_stride = cap;
         n_alloc = cap;
         return MP_OK;
     }

@@ -34,6 +34,12 @@ namespace {
 
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 
+// Resident 256-thread blocks per SM the solver kernels are compiled for
+// (caps registers at 65536 / (256 * N)).
+#ifndef MPB_SOLVER_MIN_BLOCKS
+#define MPB_SOLVER_MIN_BLOCKS 6
+#endif
+
 __device__ __forceinline__ float anchor(float o, float cs, int c) {
     return __fmaf_rn(float(c), cs, o);
 }
@@ -46,26 +52,35 @@ __device__ __forceinline__ void decode_cell(const GridDev& g, uint32_t h, int& x
     z = int(t / gy);
 }
 
-// Accumulates density, gradient sum and squared-gradient sum for one
-// candidate at offset (rx, ry, rz) (Constraints.metal:112-118).
+// In-range masks of one lambda pass.  For each particle and each of the 9
+// stencil rows, bit i is set when candidate slot b0 + i of that row lies
+// within h.  The delta pass of the same iteration sees the same positions and
+// the same stencil, hence exactly the same in-range pairs, so it walks these
+// bits instead of sweeping the 27 cells again.  Row-major layout (row r of
+// slot s at r * stride + s): the warp's stores and loads of one row coalesce.
+// A particle with a row longer than 32 candidates gets overflow[s] = 1 and is
+// swept in full by the delta pass.  rows == nullptr disables the masks.
+struct RowMasks {
+    uint32_t* rows;
+    uint32_t* overflow;
+    uint32_t stride;
+};
+
+// Density / gradient terms of one in-range candidate at offset r, r2 = |r|^2
+// < h^2 (Constraints.metal:112-118).  The particle itself (r2 = 0) adds W(0).
 struct LambdaAcc {
     float dens = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f, gsq = 0.0f;
-    uint32_t cnt = 0;
-    __device__ __forceinline__ void add(const StepConsts& c, float rx, float ry, float rz) {
-        const float r2 = dist2(rx, ry, rz);
-        if (r2 < c.h2) {
-            ++cnt;
-            const float d = c.h2 - r2;
-            dens += c.poly6 * d * d * d;
-            if (r2 > 1e-12f) {
-                const float rinv = rsqrtf(r2);
-                const float hd = fmaxf(c.h - r2 * rinv, 0.0f);
-                const float sc = -c.spiky * hd * hd * rinv;
-                gx += sc * rx;
-                gy += sc * ry;
-                gz += sc * rz;
-                gsq += sc * sc * r2;
-            }
+    __device__ __forceinline__ void add(const StepConsts& c, float rx, float ry, float rz, float r2) {
+        const float d = c.h2 - r2;
+        dens += c.poly6 * d * d * d;
+        if (r2 > 1e-12f) {
+            const float rinv = rsqrtf(r2);
+            const float hd = fmaxf(c.h - r2 * rinv, 0.0f);
+            const float sc = -c.spiky * hd * hd * rinv;
+            gx += sc * rx;
+            gy += sc * ry;
+            gz += sc * rz;
+            gsq += sc * sc * r2;
         }
     }
     __device__ __forceinline__ float lambda(const StepConsts& c) const {
@@ -75,11 +90,10 @@ struct LambdaAcc {
     }
 };
 
-// Position correction contribution of one candidate (Constraints.metal:170-181).
+// Position-correction term of one in-range candidate (Constraints.metal:170-181).
 __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float lj, float rx, float ry,
-                                          float rz, float& dx, float& dy, float& dz) {
-    const float r2 = dist2(rx, ry, rz);
-    if (r2 < c.h2 && r2 > 1e-12f) {
+                                          float rz, float r2, float& dx, float& dy, float& dz) {
+    if (r2 > 1e-12f) {
         const float d = c.h2 - r2;
         const float ratio = c.poly6 * d * d * d * c.inv_wq;
         const float scorr = -c.scorr_k * pow_n(ratio, c.scorr_n);
@@ -92,69 +106,106 @@ __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float l
     }
 }
 
-// Visit every candidate of the 27-cell stencil around the cell of the
-// particle at absolute FP32 position X (the current iterate), calling
-// f(k, ox, oy, oz) with the particle's offset from candidate k's cell anchor:
-// candidate vector r = (ox, oy, oz) - l_k.
-template <class F>
-__device__ __forceinline__ void for_stencil_anchored(const StepConsts& c, const uint32_t* cstart,
-                                                     float Xx, float Xy, float Xz, int pcx, int pcy,
-                                                     int pcz, float lx, float ly, float lz, F&& f) {
-    int cx, cy, cz;
-    cell_of(c.g, Xx, Xy, Xz, cx, cy, cz);
+// Two-phase sweep of the 27-cell stencil around cell (cx, cy, cz).  Each row
+// (3 consecutive cells, one contiguous slot range) is taken in chunks of 32
+// candidates: phase 1 loads every candidate once, does only the distance test
+// and sets a bit for each one within h; phase 2 visits just the set bits and
+// calls body(q, rx, ry, rz, r2).  The in-range body, about an eighth of the
+// candidates, then runs on most lanes of the warp instead of on the few lanes
+// whose candidate happened to be in range.
+//
+// ANCHORED = false: (px, py, pz) is the absolute FP32 position and r = p - q.
+// ANCHORED = true:  (px, py, pz) is the offset l from the anchor of hash cell
+// (pcx, pcy, pcz); r = ((A_i - A_cell(k)) + l_i) - l_k, A_i - A_cell(k) exact.
+//
+// With masks, a row that fits one chunk stores its bits (the particle's own
+// bit cleared) for the delta pass; a longer row sets the overflow flag.
+// Returns the number of in-range candidates, the particle itself included.
+template <bool ANCHORED, class Body>
+__device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __restrict__ src,
+                                          const uint32_t* __restrict__ cstart, int cx, int cy, int cz,
+                                          float px, float py, float pz, int pcx, int pcy, int pcz,
+                                          uint32_t s, const RowMasks* masks, Body&& body) {
     const int x0 = max(cx - 1, 0), x1 = min(cx + 1, c.g.gx - 1);
     const int y0 = max(cy - 1, 0), y1 = min(cy + 1, c.g.gy - 1);
     const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
-    const float aix = anchor(c.g.ox, c.g.cs, pcx), aiy = anchor(c.g.oy, c.g.cs, pcy),
-                aiz = anchor(c.g.oz, c.g.cs, pcz);
-    // the particle's x offset from the anchors of the (up to) three x cells
     const int nx = x1 - x0 + 1;
-    const float ox0 = (aix - anchor(c.g.ox, c.g.cs, x0)) + lx;
-    const float ox1 = (aix - anchor(c.g.ox, c.g.cs, x0 + 1)) + lx;
-    const float ox2 = (aix - anchor(c.g.ox, c.g.cs, x0 + 2)) + lx;
+    float ox0 = px, ox1 = px, ox2 = px;
+    float aiy = 0.0f, aiz = 0.0f;
+    if (ANCHORED) {
+        const float aix = anchor(c.g.ox, c.g.cs, pcx);
+        aiy = anchor(c.g.oy, c.g.cs, pcy);
+        aiz = anchor(c.g.oz, c.g.cs, pcz);
+        ox0 = (aix - anchor(c.g.ox, c.g.cs, x0)) + px;
+        ox1 = (aix - anchor(c.g.ox, c.g.cs, x0 + 1)) + px;
+        ox2 = (aix - anchor(c.g.ox, c.g.cs, x0 + 2)) + px;
+    }
+    uint32_t hits = 0, over = 0;
     for (int z = z0; z <= z1; ++z) {
-        const float oz = (aiz - anchor(c.g.oz, c.g.cs, z)) + lz;
+        const float oz = ANCHORED ? (aiz - anchor(c.g.oz, c.g.cs, z)) + pz : pz;
         for (int y = y0; y <= y1; ++y) {
-            const float oy = (aiy - anchor(c.g.oy, c.g.cs, y)) + ly;
-            // all cell boundaries of the row up front (independent loads)
+            const float oy = ANCHORED ? (aiy - anchor(c.g.oy, c.g.cs, y)) + py : py;
             const uint32_t base = cell_hash(c.g, x0, y, z);
             const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
             const uint32_t b2 = nx > 1 ? cstart[base + 2] : b1;
             const uint32_t b3 = nx > 2 ? cstart[base + 3] : b2;
-            for (uint32_t k = b0; k < b1; ++k) f(k, ox0, oy, oz);
-            for (uint32_t k = b1; k < b2; ++k) f(k, ox1, oy, oz);
-            for (uint32_t k = b2; k < b3; ++k) f(k, ox2, oy, oz);
+            uint32_t first = 0;  // bits of the first chunk (the whole row if b3 - b0 <= 32)
+            for (uint32_t c0 = b0; c0 < b3; c0 += 32) {
+                const uint32_t c1 = min(c0 + 32u, b3);
+                uint32_t mask = 0;
+                for (uint32_t k = c0; k < c1; ++k) {
+                    const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
+                    const float4 q = __ldg(&src[k]);
+                    const float r2 = dist2(ox - q.x, oy - q.y, oz - q.z);
+                    mask |= uint32_t(r2 < c.h2) << (k - c0);
+                }
+                if (c0 == b0) first = mask;
+                hits += __popc(mask);
+                while (mask) {
+                    const uint32_t k = c0 + uint32_t(__ffs(mask) - 1);
+                    mask &= mask - 1;
+                    const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
+                    const float4 q = __ldg(&src[k]);
+                    const float rx = ox - q.x, ry = oy - q.y, rz = oz - q.z;
+                    body(q, rx, ry, rz, dist2(rx, ry, rz));
+                }
+            }
+            if (masks) {
+                // every row of the stencil is stored, empty ones as 0
+                if (b3 - b0 <= 32u) {
+                    const uint32_t self = s - b0;
+                    masks->rows[uint32_t((z - z0) * 3 + (y - y0)) * masks->stride + s] =
+                        self < 32u ? (first & ~(1u << self)) : first;
+                } else {
+                    over = 1;
+                }
+            }
         }
     }
+    if (masks) masks->overflow[s] = over;
+    return hits;
 }
 
 // First lambda pass: absolute FP32 predicted positions (reference arithmetic,
 // so the fused neighbour count equals countNeighbors bit for bit); converts
 // the state to anchored offsets for the following passes.
 template <bool LAST>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, MPB_SOLVER_MIN_BLOCKS)
 k_lambda_first(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
                uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
                const uint32_t* __restrict__ sidx, float* __restrict__ lambdas,
-               uint32_t* __restrict__ ncount) {
+               uint32_t* __restrict__ ncount, RowMasks rm) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= c.n) return;
     const float4 p = cur[s];
     int cx, cy, cz;
     cell_of(c.g, p.x, p.y, p.z, cx, cy, cz);
-    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, c.g.gx - 1);
-    const int y0 = max(cy - 1, 0), y1 = min(cy + 1, c.g.gy - 1);
-    const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
     LambdaAcc acc;
-    for (int z = z0; z <= z1; ++z)
-        for (int y = y0; y <= y1; ++y) {
-            const uint32_t a = cstart[cell_hash(c.g, x0, y, z)];
-            const uint32_t b = cstart[cell_hash(c.g, x1, y, z) + 1];
-            for (uint32_t k = a; k < b; ++k) {
-                const float4 q = __ldg(&cur[k]);
-                acc.add(c, p.x - q.x, p.y - q.y, p.z - q.z);
-            }
-        }
+    const uint32_t cnt = sweep<false>(c, cur, cstart, cx, cy, cz, p.x, p.y, p.z, cx, cy, cz, s,
+                                      rm.rows ? &rm : nullptr,
+                                      [&](const float4&, float rx, float ry, float rz, float r2) {
+                                          acc.add(c, rx, ry, rz, r2);
+                                      });
     const float lambda = acc.lambda(c);
     // l = p - A(c): exact for the particle's own cell (Sterbenz), so the
     // anchored state starts equal to the FP32 predicted position.
@@ -165,30 +216,26 @@ k_lambda_first(StepConsts c, const float4* __restrict__ cur, float4* __restrict_
     // the particle itself was counted iff its own distance test passed
     // (false for a non-finite position)
     const uint32_t self = dist2(p.x - p.x, p.y - p.y, p.z - p.z) < c.h2 ? 1u : 0u;
-    ncount[j] = acc.cnt - self;
+    ncount[j] = cnt - self;
     if (LAST) lambdas[j] = lambda;
 }
 
 // Later lambda passes on the anchored state.
 template <bool LAST>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, MPB_SOLVER_MIN_BLOCKS)
 k_lambda(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
          const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
-         const uint32_t* __restrict__ sidx, float* __restrict__ lambdas) {
+         const uint32_t* __restrict__ sidx, float* __restrict__ lambdas, RowMasks rm) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= c.n) return;
     const float4 l = cur[s];
-    int pcx, pcy, pcz;
+    int pcx, pcy, pcz, cx, cy, cz;
     decode_cell(c.g, scell[s], pcx, pcy, pcz);
-    const float Xx = anchor(c.g.ox, c.g.cs, pcx) + l.x;
-    const float Xy = anchor(c.g.oy, c.g.cs, pcy) + l.y;
-    const float Xz = anchor(c.g.oz, c.g.cs, pcz) + l.z;
+    cell_of(c.g, anchor(c.g.ox, c.g.cs, pcx) + l.x, anchor(c.g.oy, c.g.cs, pcy) + l.y,
+            anchor(c.g.oz, c.g.cs, pcz) + l.z, cx, cy, cz);
     LambdaAcc acc;
-    for_stencil_anchored(c, cstart, Xx, Xy, Xz, pcx, pcy, pcz, l.x, l.y, l.z,
-                         [&](uint32_t k, float ox, float oy, float oz) {
-                             const float4 q = __ldg(&cur[k]);
-                             acc.add(c, ox - q.x, oy - q.y, oz - q.z);
-                         });
+    sweep<true>(c, cur, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s, rm.rows ? &rm : nullptr,
+                [&](const float4&, float rx, float ry, float rz, float r2) { acc.add(c, rx, ry, rz, r2); });
     const float lambda = acc.lambda(c);
     nxt[s] = make_float4(l.x, l.y, l.z, lambda);
     if (LAST) lambdas[sidx[s]] = lambda;
@@ -245,12 +292,12 @@ __device__ __forceinline__ void finalize_particle(const StepConsts& c, uint32_t 
 }
 
 template <bool LAST>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, MPB_SOLVER_MIN_BLOCKS)
 k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
         const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
         const uint32_t* __restrict__ sidx, const SphereState* __restrict__ sphere,
         float4* __restrict__ pos, float4* __restrict__ vel, const float4* __restrict__ prev,
-        const uint32_t* __restrict__ ncount, float* __restrict__ foam, uint32_t* err) {
+        const uint32_t* __restrict__ ncount, float* __restrict__ foam, uint32_t* err, RowMasks rm) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= c.n) return;
     const float4 l = src[s];
@@ -258,12 +305,44 @@ k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
     decode_cell(c.g, scell[s], pcx, pcy, pcz);
     const float ax = anchor(c.g.ox, c.g.cs, pcx), ay = anchor(c.g.oy, c.g.cs, pcy),
                 az = anchor(c.g.oz, c.g.cs, pcz);
+    int cx, cy, cz;
+    cell_of(c.g, ax + l.x, ay + l.y, az + l.z, cx, cy, cz);
     float dx = 0.0f, dy = 0.0f, dz = 0.0f;
-    for_stencil_anchored(c, cstart, ax + l.x, ay + l.y, az + l.z, pcx, pcy, pcz, l.x, l.y, l.z,
-                         [&](uint32_t k, float ox, float oy, float oz) {
-                             const float4 q = __ldg(&src[k]);
-                             delta_add(c, l.w, q.w, ox - q.x, oy - q.y, oz - q.z, dx, dy, dz);
-                         });
+    auto body = [&](const float4& q, float rx, float ry, float rz, float r2) {
+        delta_add(c, l.w, q.w, rx, ry, rz, r2, dx, dy, dz);
+    };
+    if (rm.rows != nullptr && rm.overflow[s] == 0u) {
+        // the lambda pass's in-range bits, row by row (rows fit one chunk)
+        const int x0 = max(cx - 1, 0), x1 = min(cx + 1, c.g.gx - 1);
+        const int y0 = max(cy - 1, 0), y1 = min(cy + 1, c.g.gy - 1);
+        const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
+        const int nx = x1 - x0 + 1;
+        const float ox0 = (ax - anchor(c.g.ox, c.g.cs, x0)) + l.x;
+        const float ox1 = (ax - anchor(c.g.ox, c.g.cs, x0 + 1)) + l.x;
+        const float ox2 = (ax - anchor(c.g.ox, c.g.cs, x0 + 2)) + l.x;
+        for (int z = z0; z <= z1; ++z) {
+            const float oz = (az - anchor(c.g.oz, c.g.cs, z)) + l.z;
+            for (int y = y0; y <= y1; ++y) {
+                uint32_t mask = rm.rows[uint32_t((z - z0) * 3 + (y - y0)) * rm.stride + s];
+                if (mask == 0u) continue;
+                const float oy = (ay - anchor(c.g.oy, c.g.cs, y)) + l.y;
+                const uint32_t base = cell_hash(c.g, x0, y, z);
+                const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
+                const uint32_t b2 = nx > 1 ? cstart[base + 2] : b1;
+                while (mask) {
+                    const uint32_t k = b0 + uint32_t(__ffs(mask) - 1);
+                    mask &= mask - 1;
+                    const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
+                    const float4 q = __ldg(&src[k]);
+                    const float rx = ox - q.x, ry = oy - q.y, rz = oz - q.z;
+                    body(q, rx, ry, rz, dist2(rx, ry, rz));
+                }
+            }
+        }
+    } else {
+        sweep<true>(c, src, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s,
+                    static_cast<const RowMasks*>(nullptr), body);
+    }
     dx *= c.inv_rho0;
     dy *= c.inv_rho0;
     dz *= c.inv_rho0;
@@ -328,29 +407,30 @@ cudaError_t launch_solver(const StepConsts& c, const DevState& d, uint32_t itera
         tend(t, "finalize", s);
         return cudaGetLastError();
     }
+    const RowMasks rm{d.row_masks, d.mask_overflow, d.mask_stride};  // 9 x u32 per slot
     for (uint32_t it = 0; it < iterations; ++it) {
         const bool first = it == 0, last = it + 1 == iterations;
         tbegin(t, s);
         if (first && last)
             k_lambda_first<true><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart,
-                                                      d.sidx, d.lambdas, d.ncount);
+                                                      d.sidx, d.lambdas, d.ncount, rm);
         else if (first)
             k_lambda_first<false><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart,
-                                                       d.sidx, d.lambdas, d.ncount);
+                                                       d.sidx, d.lambdas, d.ncount, rm);
         else if (last)
             k_lambda<true><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart, d.sidx,
-                                                d.lambdas);
+                                                d.lambdas, rm);
         else
             k_lambda<false><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart, d.sidx,
-                                                 d.lambdas);
+                                                 d.lambdas, rm);
         tend(t, first ? "lambda_count" : "lambda", s);
         tbegin(t, s);
         if (last)
             k_delta<true><<<grid, 256, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
-                                               d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err);
+                                               d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
         else
             k_delta<false><<<grid, 256, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
-                                                d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err);
+                                                d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
         tend(t, last ? "delta_finalize" : "delta", s);
     }
     return cudaGetLastError();
