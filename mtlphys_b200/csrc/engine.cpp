@@ -88,9 +88,11 @@ int make_grid(const mp_pbf_params& p, GridDev& g) {
     g.oz = p.bounds_min[2];
     g.inv = 1.0f / p.cell_size;
     g.cs = p.cell_size;
-    g.gx = int(dims[0]);
-    g.gy = int(dims[1]);
-    g.gz = int(dims[2]);
+    g.gx = g.dgx = int(dims[0]);
+    g.gy = g.dgy = int(dims[1]);
+    g.gz = g.dgz = int(dims[2]);
+    g.lx = g.ly = g.lz = 0;
+    g.cell0 = 0;
     g.cells = uint32_t(cells);
     return MP_OK;
 }

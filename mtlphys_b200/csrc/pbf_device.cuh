@@ -17,13 +17,22 @@
 
 namespace mpb {
 
-// Uniform hash grid: SpatialParams (engine/shaders/Shared.h:40-49).
+// Uniform hash grid: SpatialParams (engine/shaders/Shared.h:40-49).  A
+// particle's cell is computed on the dense grid (origin, cell size, dense
+// dims) exactly as the reference does; the cells that are stored may be a
+// box-shaped sub-grid of it (lower corner l, dims g, stored from cell0 on),
+// with the same x-fastest order, so the sorted order does not change.  The
+// single-scene engine stores the whole dense grid (l = 0, g = dense dims,
+// cell0 = 0); the batched engine stores each scene's bounding box of cells.
 struct GridDev {
-    float ox, oy, oz;  // gridOrigin (= bounds_min)
-    float inv;         // invCellSize = 1.0f / cellSize, rounded on the host
-    float cs;          // cellSize
-    int gx, gy, gz;    // gridDim
-    uint32_t cells;    // gx * gy * gz
+    float ox, oy, oz;    // gridOrigin (= bounds_min)
+    float inv;           // invCellSize = 1.0f / cellSize, rounded on the host
+    float cs;            // cellSize
+    int dgx, dgy, dgz;   // dense gridDim: cell coordinates are clamped to it
+    int lx, ly, lz;      // sub-grid lower corner, in dense cell coordinates
+    int gx, gy, gz;      // sub-grid dims
+    uint32_t cell0;      // index of the sub-grid's first cell in the cell arrays
+    uint32_t cells;      // gx * gy * gz
 };
 
 // Per-launch constants of one step (PBFParams, Shared.h:53-71, plus the
@@ -69,15 +78,42 @@ __device__ __forceinline__ int cell_axis(float p, float o, float inv, int dim) {
     return min(max(c, 0), dim - 1);
 }
 
-__device__ __forceinline__ uint32_t cell_hash(const GridDev& g, int x, int y, int z) {
+// Linear id of sub-grid cell (x, y, z), x fastest (cellHashOf).
+__device__ __forceinline__ uint32_t cell_local(const GridDev& g, int x, int y, int z) {
     return uint32_t(x) + uint32_t(y) * uint32_t(g.gx) + uint32_t(z) * uint32_t(g.gx) * uint32_t(g.gy);
 }
 
+// Index of sub-grid cell (x, y, z) in the cell arrays.
+__device__ __forceinline__ uint32_t cell_hash(const GridDev& g, int x, int y, int z) {
+    return g.cell0 + cell_local(g, x, y, z);
+}
+
+// Cell of a position, in sub-grid coordinates (inside the sub-grid for every
+// position its bounding box was built from).
 __device__ __forceinline__ void cell_of(const GridDev& g, float px, float py, float pz, int& cx,
                                         int& cy, int& cz) {
-    cx = cell_axis(px, g.ox, g.inv, g.gx);
-    cy = cell_axis(py, g.oy, g.inv, g.gy);
-    cz = cell_axis(pz, g.oz, g.inv, g.gz);
+    cx = cell_axis(px, g.ox, g.inv, g.dgx) - g.lx;
+    cy = cell_axis(py, g.oy, g.inv, g.dgy) - g.ly;
+    cz = cell_axis(pz, g.oz, g.inv, g.dgz) - g.lz;
+}
+
+__device__ __forceinline__ void decode_cell(const GridDev& g, uint32_t local, int& x, int& y, int& z) {
+    const uint32_t gx = uint32_t(g.gx), gy = uint32_t(g.gy);
+    x = int(local % gx);
+    const uint32_t t = local / gx;
+    y = int(t % gy);
+    z = int(t / gy);
+}
+
+// Lower corner of sub-grid cell index c along one axis: origin + (l + c) * cellSize.
+__device__ __forceinline__ float anchor_x(const GridDev& g, int c) {
+    return __fmaf_rn(float(c + g.lx), g.cs, g.ox);
+}
+__device__ __forceinline__ float anchor_y(const GridDev& g, int c) {
+    return __fmaf_rn(float(c + g.ly), g.cs, g.oy);
+}
+__device__ __forceinline__ float anchor_z(const GridDev& g, int c) {
+    return __fmaf_rn(float(c + g.lz), g.cs, g.oz);
 }
 
 // Squared distance with one fixed rounding order, shared by the neighbour

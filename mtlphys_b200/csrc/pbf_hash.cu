@@ -16,49 +16,12 @@
 //                           atomics), and gathers the sorted positions
 //   countNeighbors          only for the standalone buildSpatialHash; the step
 //                           fuses the count into its first lambda pass.
-#include "pbf_kernels.h"
+#include "pbf_items.cuh"
 
 namespace mpb {
 namespace {
 
-constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait (~0.1-1 s)
-
-__device__ __forceinline__ unsigned lanemask_lt() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-// Engine.cpp:694-707 (host-side sphere kinematics in the reference), in FP32
-// with one rounding per operation, run by one thread before the hash.
-__device__ void sphere_advance(const StepConsts& c, SphereState* s) {
-    float vx = s->v[0], vy = s->v[1], vz = s->v[2];
-    vy = __fadd_rn(vy, __fmul_rn(c.sph_gravity, c.dt));
-    vx = __fmul_rn(vx, c.sph_drag);
-    vy = __fmul_rn(vy, c.sph_drag);
-    vz = __fmul_rn(vz, c.sph_drag);
-    float p[3] = {__fadd_rn(s->c[0], __fmul_rn(vx, c.dt)), __fadd_rn(s->c[1], __fmul_rn(vy, c.dt)),
-                  __fadd_rn(s->c[2], __fmul_rn(vz, c.dt))};
-    float v[3] = {vx, vy, vz};
-    const float lo[3] = {c.bminx, c.bminy, c.bminz};
-    const float hi[3] = {c.bmaxx, c.bmaxy, c.bmaxz};
-    const float r = s->r;
-    for (int a = 0; a < 3; ++a) {
-        if (__fsub_rn(p[a], r) < lo[a]) {
-            p[a] = __fadd_rn(lo[a], r);
-            v[a] = __fmul_rn(-v[a], c.sph_rest);
-        }
-        if (__fadd_rn(p[a], r) > hi[a]) {
-            p[a] = __fsub_rn(hi[a], r);
-            v[a] = __fmul_rn(-v[a], c.sph_rest);
-        }
-    }
-    for (int a = 0; a < 3; ++a) {
-        s->c[a] = p[a];
-        s->v[a] = v[a];
-    }
-}
 
 // predictPositions (Constraints.metal:54-66) + hashCells (Spatial.metal:49-57)
 // + countCells (Spatial.metal:63-70) in one pass.
@@ -75,38 +38,15 @@ k_predict_hash(StepConsts c, float4* __restrict__ pos, const float4* __restrict_
     const bool active = i < c.n;
     uint32_t cell = 0;
     if (active) {
-        float4 p = pos[i];
-        if (predict) {
-            const float4 v = vel[i];
-            // A non-finite input survives as a finite clamped position (the
-            // reference's clamp semantics), so flag it here, on entry.
-            if (!isfinite(p.x + p.y + p.z + v.x + v.y + v.z)) atomicOr(err, kDevErrNaN);
-            prev[i] = p;
-            // v' = v + g*dt and p' = p + v'*dt, each one fused multiply-add.
-            const float vx = __fmaf_rn(c.gravx, c.dt, v.x);
-            const float vy = __fmaf_rn(c.gravy, c.dt, v.y);
-            const float vz = __fmaf_rn(c.gravz, c.dt, v.z);
-            p.x = __fmaf_rn(vx, c.dt, p.x);
-            p.y = __fmaf_rn(vy, c.dt, p.y);
-            p.z = __fmaf_rn(vz, c.dt, p.z);
-            pos[i] = p;
-        }
+        const float4 p = predict ? predict_item(c, i, pos, vel, prev, err) : pos[i];
         int cx, cy, cz;
         cell_of(c.g, p.x, p.y, p.z, cx, cy, cz);
         cell = cell_hash(c.g, cx, cy, cz);
         hash[i] = cell;
     }
-    // Warp-aggregated count: one atomic per distinct cell in the warp.
-    const unsigned act = __ballot_sync(kFull, active);
-    if (active) {
-        const unsigned peers = __match_any_sync(act, cell);
-        const int leader = __ffs(peers) - 1;
-        const int lane = threadIdx.x & 31;
-        uint32_t base = 0;
-        if (lane == leader) base = atomicAdd(&counts[cell], uint32_t(__popc(peers)));
-        base = __shfl_sync(act, base, leader);
-        off[i] = base + uint32_t(__popc(peers & lanemask_lt()));
-    }
+    uint32_t rank = 0;
+    count_cell(active, cell, counts, &rank);
+    if (active) off[i] = rank;
 }
 
 // ---- single-pass exclusive scan (decoupled look-back) -----------------------
@@ -262,41 +202,23 @@ k_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status
     }
 }
 
-// scatterParticles (Spatial.metal:169-180) without the second atomic: the
-// rank came from the counting pass.
 __global__ void __launch_bounds__(256)
 k_scatter(uint32_t n, const uint32_t* __restrict__ hash, const uint32_t* __restrict__ off,
           const uint32_t* __restrict__ cstart, uint32_t* __restrict__ tmp) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    tmp[cstart[hash[i]] + off[i]] = i;
+    if (i < n) scatter_item(i, hash, off, cstart, tmp);
 }
 
-// Stable re-rank inside the cell segment + gatherPositions (Spatial.metal:
-// 190-198).  Segments longer than kSegMax are queued for k_long_segments.
 __global__ void __launch_bounds__(256)
 k_sort_gather(uint32_t n, const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ hash,
               const uint32_t* __restrict__ cstart, const float4* __restrict__ pos,
               uint32_t* __restrict__ sidx, float4* __restrict__ sorted,
               uint32_t* __restrict__ long_list, uint32_t* __restrict__ long_count) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const uint32_t j = tmp[s];
-    const uint32_t c = hash[j];
-    const uint32_t a = cstart[c], b = cstart[c + 1];
-    if (b - a > kSegMax) {
-        if (s == a) long_list[atomicAdd(long_count, 1u)] = c;
-        return;
-    }
-    uint32_t rank = 0;
-    for (uint32_t k = a; k < b; ++k) rank += (tmp[k] < j) ? 1u : 0u;
-    const uint32_t d = a + rank;
-    sidx[d] = j;
-    sorted[d] = pos[j];
+    if (s < n) sort_gather_item(s, tmp, hash, cstart, pos, sidx, sorted, long_list, long_count);
 }
 
-// Long segments: rank(j) = number of particles j' < j in the same cell, from
-// a block-wide scan over all particle indices.  One block per queued cell.
+// One block per queued long segment.
 __global__ void __launch_bounds__(256)
 k_long_segments(uint32_t n, const uint32_t* __restrict__ hash, const uint32_t* __restrict__ cstart,
                 const float4* __restrict__ pos, uint32_t* __restrict__ sidx,
@@ -304,61 +226,16 @@ k_long_segments(uint32_t n, const uint32_t* __restrict__ hash, const uint32_t* _
                 const uint32_t* __restrict__ long_count) {
     __shared__ uint32_t s_warp[8];
     const uint32_t total = *long_count;
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (uint32_t li = blockIdx.x; li < total; li += gridDim.x) {
-        const uint32_t c = long_list[li];
-        const uint32_t a = cstart[c], len = cstart[c + 1] - a;
-        uint32_t running = 0;
-        for (uint32_t base = 0; base < n && running < len; base += blockDim.x) {
-            const uint32_t j = base + threadIdx.x;
-            const bool f = j < n && hash[j] == c;
-            const unsigned m = __ballot_sync(kFull, f);
-            if (lane == 0) s_warp[warp] = __popc(m);
-            __syncthreads();
-            uint32_t before = 0, blk = 0;
-            for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
-                if (w < warp) before += s_warp[w];
-                blk += s_warp[w];
-            }
-            if (f) {
-                const uint32_t d = a + running + before + __popc(m & lanemask_lt());
-                sidx[d] = j;
-                sorted[d] = pos[j];
-            }
-            running += blk;
-            __syncthreads();
-        }
-    }
+    for (uint32_t li = blockIdx.x; li < total; li += gridDim.x)
+        long_segment(long_list[li], 0u, n, hash, cstart, pos, sidx, sorted, s_warp);
 }
 
-// countNeighbors (Spatial.metal:207-243) in sorted order: the 27-cell
-// stencil is 9 contiguous slot ranges (x-fastest hash).
 __global__ void __launch_bounds__(256)
 k_count_neighbors(StepConsts c, const float4* __restrict__ sorted,
                   const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ sidx,
                   uint32_t* __restrict__ ncount) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= c.n) return;
-    const float4 p = sorted[s];
-    int cx, cy, cz;
-    cell_of(c.g, p.x, p.y, p.z, cx, cy, cz);
-    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, c.g.gx - 1);
-    const int y0 = max(cy - 1, 0), y1 = min(cy + 1, c.g.gy - 1);
-    const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
-    uint32_t cnt = 0;
-    for (int z = z0; z <= z1; ++z)
-        for (int y = y0; y <= y1; ++y) {
-            const uint32_t a = cstart[cell_hash(c.g, x0, y, z)];
-            const uint32_t b = cstart[cell_hash(c.g, x1, y, z) + 1];
-            for (uint32_t k = a; k < b; ++k) {
-                const float4 q = __ldg(&sorted[k]);
-                const float r2 = dist2(q.x - p.x, q.y - p.y, q.z - p.z);
-                cnt += (r2 < c.h2) ? 1u : 0u;
-            }
-        }
-    // the particle itself passed its own distance test unless its position is
-    // not finite
-    ncount[sidx[s]] = cnt - (dist2(p.x - p.x, p.y - p.y, p.z - p.z) < c.h2 ? 1u : 0u);
+    if (s < c.n) count_neighbors_item(c, s, sorted, cstart, sidx, ncount);
 }
 
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
