@@ -208,6 +208,54 @@ int mp_engine_get_sphere(mp_engine* e, float center[3], float velocity[3], float
 int mp_engine_check_errors(mp_engine* e, uint32_t* bits);
 int mp_engine_synchronize(mp_engine* e);
 
+/* ---- batch of independent scenes (no reference counterpart: the reference
+ *      steps one scene per Engine) -------------------------------------------
+ * All scenes advance in one persistent, cooperative launch per step (or, in
+ * serial mode, the same kernel launched once per scene).  Each scene has its
+ * own parameters, dt, seeding and sphere, and gives the results a
+ * single-scene engine would give (the same particle order and arithmetic).
+ * Particles of scene s are the contiguous range mp_batch_scene_range(s) of
+ * the batch's buffers (MP_BUF_* as for an engine; MP_BUF_CELL_START holds the
+ * scenes' bounding boxes of cells laid end to end). */
+typedef struct mp_batch mp_batch;
+typedef struct mp_batch_tuning {
+    uint32_t block;          /* threads per block: 128, 256 or 512     */
+    uint32_t blocks_per_sm;  /* resident blocks per SM of the launch   */
+    float    ms_per_step;    /* measured by mp_batch_autotune          */
+} mp_batch_tuning;
+int mp_batch_create(int device, mp_batch** out);
+int mp_batch_destroy(mp_batch* b);
+/* nscenes scenes: counts[s] particles, scene_ids[s] (MP_SCENE_*, NULL = cube
+ * drop), params[s], descs[s] (NULL = reference placement), dts[s] > 0.  All
+ * scenes use the same solver_iterations. */
+int mp_batch_reset(mp_batch* b, uint32_t nscenes, const uint32_t* counts, const uint32_t* scene_ids,
+                   const mp_pbf_params* params, const mp_scene_desc* descs, const float* dts);
+int mp_batch_set_dts(mp_batch* b, const float* dts);
+/* One step of every scene, asynchronous on `stream`. */
+int mp_batch_step(mp_batch* b, mp_stream stream);
+/* 0: one launch for all scenes (default); 1: the same kernel once per scene. */
+int mp_batch_set_mode(mp_batch* b, int serial);
+/* Capture a step into a CUDA graph and replay it (1), or launch directly (0). */
+int mp_batch_set_graph_mode(mp_batch* b, int enable);
+/* Launch shape (block = 128/256/512, blocks_per_sm 0 = as many as fit). */
+int mp_batch_set_launch(mp_batch* b, uint32_t block, uint32_t blocks_per_sm);
+int mp_batch_get_launch(const mp_batch* b, uint32_t* block, uint32_t* blocks);
+/* Time `steps` steps for every launch shape from the same saved state
+ * (restored afterwards), keep the fastest, and remember it for batches of
+ * the same scene count and particle-count bucket.  Results are identical for
+ * every shape. */
+int mp_batch_autotune(mp_batch* b, uint32_t steps, mp_batch_tuning* best);
+uint32_t mp_batch_scene_count(const mp_batch* b);
+uint32_t mp_batch_particle_count(const mp_batch* b);
+int mp_batch_scene_range(const mp_batch* b, uint32_t scene, uint32_t* first, uint32_t* count);
+int mp_batch_buffer(mp_batch* b, uint32_t which, void** dptr, size_t* bytes);
+int mp_batch_upload(mp_batch* b, uint32_t which, const void* host, size_t count, mp_stream stream);
+int mp_batch_download(mp_batch* b, uint32_t which, void* host, size_t count, mp_stream stream);
+int mp_batch_set_sphere(mp_batch* b, uint32_t scene, const float center[3], const float velocity[3],
+                        float radius);
+int mp_batch_get_sphere(mp_batch* b, uint32_t scene, float center[3], float velocity[3], float* radius);
+int mp_batch_check_errors(mp_batch* b, uint32_t* bits);
+
 /* ---- scan: Engine.hpp:92-100 --------------------------------------------- */
 /* runExclusiveScan(cmd, in, out, chunkSums, n) (Engine.cpp:843-882): out[i]
  * = sum of in[0..i) modulo 2^32, single pass with decoupled look-back; no

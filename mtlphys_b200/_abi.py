@@ -121,6 +121,12 @@ class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint32), ("ms", C.c_double)]
 
 
+class BatchTuning(C.Structure):
+    """mp_batch_tuning."""
+
+    _fields_ = [("block", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("ms_per_step", C.c_float)]
+
+
 _VP = C.c_void_p
 _U32 = C.c_uint32
 _INT = C.c_int
@@ -158,6 +164,27 @@ PROTOTYPES = {
                                     C.POINTER(C.c_float)]),
     "mp_engine_check_errors": (_INT, [_VP, C.POINTER(_U32)]),
     "mp_engine_synchronize": (_INT, [_VP]),
+    "mp_batch_create": (_INT, [_INT, C.POINTER(_VP)]),
+    "mp_batch_destroy": (_INT, [_VP]),
+    "mp_batch_reset": (_INT, [_VP, _U32, C.POINTER(_U32), C.POINTER(_U32), C.POINTER(PBFParams),
+                              C.POINTER(SceneDesc), C.POINTER(C.c_float)]),
+    "mp_batch_set_dts": (_INT, [_VP, C.POINTER(C.c_float)]),
+    "mp_batch_step": (_INT, [_VP, _VP]),
+    "mp_batch_set_mode": (_INT, [_VP, _INT]),
+    "mp_batch_set_graph_mode": (_INT, [_VP, _INT]),
+    "mp_batch_set_launch": (_INT, [_VP, _U32, _U32]),
+    "mp_batch_get_launch": (_INT, [_VP, C.POINTER(_U32), C.POINTER(_U32)]),
+    "mp_batch_autotune": (_INT, [_VP, _U32, C.POINTER(BatchTuning)]),
+    "mp_batch_scene_count": (_U32, [_VP]),
+    "mp_batch_particle_count": (_U32, [_VP]),
+    "mp_batch_scene_range": (_INT, [_VP, _U32, C.POINTER(_U32), C.POINTER(_U32)]),
+    "mp_batch_buffer": (_INT, [_VP, _U32, C.POINTER(_VP), C.POINTER(_SZ)]),
+    "mp_batch_upload": (_INT, [_VP, _U32, _VP, _SZ, _VP]),
+    "mp_batch_download": (_INT, [_VP, _U32, _VP, _SZ, _VP]),
+    "mp_batch_set_sphere": (_INT, [_VP, _U32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_float]),
+    "mp_batch_get_sphere": (_INT, [_VP, _U32, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float)]),
+    "mp_batch_check_errors": (_INT, [_VP, C.POINTER(_U32)]),
     "mp_exclusive_scan_scratch_bytes": (_SZ, [_U32]),
     "mp_exclusive_scan": (_INT, [_VP, _VP, _U32, _VP, _SZ, _VP]),
     "mp_exclusive_scan_noalloc": (_INT, [_VP, _VP, _U32, _VP]),

@@ -95,3 +95,73 @@ def batch_counts(num: int, lo: int, hi: int, seed: int) -> np.ndarray:
 
 
 WORKLOADS = {"cube_drop": cube_drop, "dam_break": dam_break, "diff_cube": diff_cube}
+
+
+class BatchWorkload:
+    """Scenes of a batch: per-scene counts, parameters, dts, scene ids, descs."""
+
+    def __init__(self, name, counts, params, dts, scenes, descs, steps, spheres=None):
+        self.name, self.counts, self.params, self.dts = name, counts, params, dts
+        self.scenes, self.descs, self.steps, self.spheres = scenes, descs, steps, spheres
+
+    @property
+    def n(self) -> int:
+        return int(sum(self.counts))
+
+    def describe(self) -> dict:
+        return {"workload": self.name, "scenes": len(self.counts), "particles": self.n,
+                "min_scene": int(min(self.counts)), "max_scene": int(max(self.counts)),
+                "solver_iterations": int(self.params[0].solver_iterations), "steps": self.steps}
+
+
+def batch_cubes(num: int = 256, lo: int = 2000, hi: int = 64000, steps: int = 100) -> BatchWorkload:
+    """Independent cube drops: counts log-uniform in [lo, hi], cube side
+    ceil(cbrt(n)) (Engine.cpp:531) at the cube-drop corner (20h, 30h, 20h) of
+    the 86h box, jitter +-0.01h, per-scene dt ~ U[1/240, 1/120] and
+    epsilon ~ U[50, 200], other parameters as the cube drop."""
+    rng = np.random.Generator(np.random.MT19937(SEED_BASE + 3))
+    counts = np.exp(rng.uniform(math.log(lo), math.log(hi), size=num)).astype(np.int64)
+    dts = rng.uniform(1.0 / 240.0, 1.0 / 120.0, size=num)
+    eps = rng.uniform(50.0, 200.0, size=num)
+    params, descs = [], []
+    for s in range(num):
+        p = base_params(3)
+        p.epsilon = float(eps[s])
+        params.append(p)
+        side = int(math.ceil(round(counts[s] ** (1.0 / 3.0), 9)))
+        while side ** 3 < counts[s]:
+            side += 1
+        descs.append(lattice((side, side, side), (20 * H, 30 * H, 20 * H), SEED_BASE + 3 + 1000 * (s + 1)))
+    return BatchWorkload("batch_cubes", [int(c) for c in counts], params, [float(d) for d in dts],
+                         [_abi.MP_SCENE_CUBE_DROP] * num, descs, steps)
+
+
+def batch_spheres(num: int = 32, lo: int = 20000, hi: int = 200000, steps: int = 40) -> BatchWorkload:
+    """Sphere drops into pre-settled lakes: counts log-uniform in [lo, hi];
+    each lake is 20h deep (40 layers at 0.5h) on a square footprint sized to
+    its count, in a box whose walls hug the footprint and are 40h high; a
+    kinematic sphere of radius 8h (scaled down on footprints narrower than
+    2.5 x 16h) starts at height 35h over the centre with vertical speed
+    v0 ~ U[0, 3] m/s (downwards).  dt = 1/120, 3 iterations."""
+    rng = np.random.Generator(np.random.MT19937(SEED_BASE + 4))
+    counts = np.exp(rng.uniform(math.log(lo), math.log(hi), size=num)).astype(np.int64)
+    v0 = rng.uniform(0.0, 3.0, size=num)
+    params, descs, spheres = [], [], []
+    sp = 0.5 * H
+    for s in range(num):
+        layers = 40
+        side = int(math.ceil(math.sqrt(counts[s] / layers)))
+        width = (side - 1) * sp + 2 * 0.5 * H
+        p = base_params(3)
+        p.set(bounds_min=(0.0, 0.0, 0.0), bounds_max=(width, 40 * H, width))
+        radius = 8 * H * min(1.0, width / (2.5 * 16 * H))
+        p.sphere_radius = radius
+        params.append(p)
+        d = lattice((side, layers, side), (0.5 * H, 0.5 * H, 0.5 * H), SEED_BASE + 4 + 1000 * (s + 1))
+        d.sphere_center[0] = d.sphere_center[2] = 0.5 * width
+        d.sphere_center[1] = 35 * H
+        d.sphere_velocity[1] = -float(v0[s])
+        descs.append(d)
+        spheres.append((0.5 * width, 35 * H, 0.5 * width, 0.0, -float(v0[s]), 0.0, radius))
+    return BatchWorkload("batch_spheres", [int(c) for c in counts], params, [1.0 / 120.0] * num,
+                         [_abi.MP_SCENE_SPHERE_DROP] * num, descs, steps, spheres)

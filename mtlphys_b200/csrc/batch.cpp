@@ -1,0 +1,559 @@
+// batch.cpp — host side of the multi-scene batch (mp_batch_* in
+// include/mtlphys_b200.h): buffers for all scenes, scene seeding, the
+// per-step cooperative launch (optionally captured in a CUDA graph), the
+// scene-by-scene serial mode and the launch-shape autotuner.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <vector>
+
+#include "../../include/mtlphys_b200.h"
+#include "host_common.h"
+#include "pbf_batch.h"
+#include "pbf_kernels.h"
+
+using namespace mpb;
+
+namespace {
+
+struct TuneKey {
+    uint32_t n_bucket, scenes;
+    bool operator<(const TuneKey& o) const {
+        return n_bucket != o.n_bucket ? n_bucket < o.n_bucket : scenes < o.scenes;
+    }
+};
+// Autotuned launch shapes, per particle-count bucket (power of two) and scene count.
+std::mutex g_tune_lock;
+std::map<TuneKey, std::pair<uint32_t, uint32_t>> g_tune_cache;
+
+uint32_t pow2_bucket(uint32_t n) {
+    uint32_t b = 1;
+    while (b < n && b < (1u << 31)) b <<= 1;
+    return b;
+}
+
+}  // namespace
+
+struct mp_batch {
+    int device = 0;
+    uint32_t S = 0, N = 0, n_alloc = 0, iterations = 0;
+    std::vector<uint32_t> counts, p0, scene_ids;
+    std::vector<mp_pbf_params> params;
+    std::vector<float> dts;
+    std::vector<SceneDev> host_scenes;
+    uint32_t max_cells = 0;
+    // device memory
+    void* particle_block = nullptr;
+    void* cell_block = nullptr;
+    void* small_block = nullptr;
+    SceneDev* scenes = nullptr;
+    BatchArgs a{};
+    // launch shape / modes
+    uint32_t block = 256, blocks_per_sm = 0;
+    bool serial = false, graph_mode = false;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+
+    void drop_graph() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        gexec = nullptr;
+        graph = nullptr;
+    }
+    void free_all() {
+        drop_graph();
+        for (void* p : {particle_block, cell_block, small_block, static_cast<void*>(scenes)})
+            if (p) cudaFree(p);
+        particle_block = cell_block = small_block = nullptr;
+        scenes = nullptr;
+        a = BatchArgs{};
+    }
+    ~mp_batch() {
+        DeviceGuard g(device);
+        free_all();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+    }
+
+    uint32_t blocks() const {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int occ = batch_max_blocks_per_sm(block);
+        const int per_sm = blocks_per_sm ? std::min<int>(int(blocks_per_sm), occ) : occ;
+        return uint32_t(std::max(1, per_sm) * std::max(1, sms));
+    }
+
+    int enqueue(cudaStream_t s) {
+        if (N == 0) return MP_OK;
+        const uint32_t nb = blocks();
+        if (!serial) {
+            BatchArgs args = a;
+            args.scene_begin = 0;
+            args.scene_end = S;
+            args.p_begin = 0;
+            args.p_end = N;
+            const cudaError_t e = launch_batch_step(args, block, nb, s);
+            if (e != cudaSuccess) return fail(MP_ERR_CUDA, "batch step launch: %s", cudaGetErrorString(e));
+            return MP_OK;
+        }
+        for (uint32_t sc = 0; sc < S; ++sc) {  // the same kernel, one scene per launch
+            if (counts[sc] == 0) continue;
+            BatchArgs args = a;
+            args.scene_begin = sc;
+            args.scene_end = sc + 1;
+            args.p_begin = p0[sc];
+            args.p_end = p0[sc] + counts[sc];
+            const cudaError_t e = launch_batch_step(args, block, nb, s);
+            if (e != cudaSuccess) return fail(MP_ERR_CUDA, "batch step launch: %s", cudaGetErrorString(e));
+        }
+        return MP_OK;
+    }
+
+    int upload_scenes() {
+        MP_CUDA(cudaMemcpy(scenes, host_scenes.data(), sizeof(SceneDev) * S, cudaMemcpyHostToDevice));
+        return MP_OK;
+    }
+};
+
+namespace {
+
+int batch_buffer(mp_batch* b, uint32_t which, void** dptr, size_t* bytes) {
+    if (!b || !dptr) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    void* p = nullptr;
+    size_t count = b->N;
+    switch (which) {
+        case MP_BUF_POSITIONS: p = b->a.pos; break;
+        case MP_BUF_VELOCITIES: p = b->a.vel; break;
+        case MP_BUF_PREV_POSITIONS: p = b->a.prev; break;
+        case MP_BUF_CELL_HASHES: p = b->a.hash; break;
+        case MP_BUF_CELL_START: p = b->a.cstart; count = size_t(b->max_cells) + 1; break;
+        case MP_BUF_SORTED_INDEX: p = b->a.sidx; break;
+        case MP_BUF_NEIGHBOR_COUNTS: p = b->a.ncount; break;
+        case MP_BUF_LAMBDAS: p = b->a.lambdas; break;
+        case MP_BUF_FOAM: p = b->a.foam; break;
+        case MP_BUF_SORTED_POSITIONS: p = b->a.sorted_a; break;
+        default: return fail(MP_ERR_INVALID_ARGUMENT, "unknown buffer %u", which);
+    }
+    *dptr = p;
+    if (bytes) *bytes = count * elem_bytes(which);
+    return MP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mp_batch_create(int device, mp_batch** out) {
+    if (!out) return fail(MP_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    MP_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count)
+        return fail(MP_ERR_INVALID_ARGUMENT, "device %d not in [0, %d)", device, count);
+    int coop = 0;
+    MP_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    if (!coop) return fail(MP_ERR_UNSUPPORTED, "device %d has no cooperative launch", device);
+    auto* b = new (std::nothrow) mp_batch();
+    if (!b) return fail(MP_ERR_OUT_OF_MEMORY, "host allocation failed");
+    b->device = device;
+    *out = b;
+    return MP_OK;
+}
+
+int mp_batch_destroy(mp_batch* b) {
+    delete b;
+    return MP_OK;
+}
+
+int mp_batch_reset(mp_batch* b, uint32_t nscenes, const uint32_t* counts, const uint32_t* scene_ids,
+                   const mp_pbf_params* params, const mp_scene_desc* descs, const float* dts) {
+    if (!b || (nscenes && (!counts || !params || !dts)))
+        return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    uint64_t total = 0;
+    const uint32_t iters = nscenes ? params[0].solver_iterations : 0;
+    uint64_t worst_cells = 0;
+    std::vector<GridDev> grids(nscenes);
+    for (uint32_t s = 0; s < nscenes; ++s) {
+        int rc = validate_params(params[s]);
+        if (rc != MP_OK) return rc;
+        if (params[s].solver_iterations != iters)
+            return fail(MP_ERR_INVALID_ARGUMENT, "all scenes must use the same solver_iterations");
+        if (!(dts[s] > 0.0f)) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u: dt must be > 0", s);
+        if (scene_ids && scene_ids[s] > MP_SCENE_SPHERE_DROP)
+            return fail(MP_ERR_INVALID_ARGUMENT, "scene %u: unknown scene id %u", s, scene_ids[s]);
+        if (descs && descs[s].size != sizeof(mp_scene_desc))
+            return fail(MP_ERR_INVALID_ARGUMENT, "scene %u: mp_scene_desc.size mismatch", s);
+        rc = make_grid(params[s], grids[s]);
+        if (rc != MP_OK) return rc;
+        total += counts[s];
+        worst_cells += grids[s].cells;
+    }
+    if (total >= (1ull << 31)) return fail(MP_ERR_INVALID_ARGUMENT, "too many particles");
+    if (worst_cells >= (1ull << 31) - 1) return fail(MP_ERR_INVALID_ARGUMENT, "scene grids too large");
+    // seed every scene on the host
+    std::vector<float> pos(4 * size_t(total), 0.0f), tmp;
+    std::vector<uint32_t> scene_of(total);
+    std::vector<SceneDev> hs(nscenes);
+    uint64_t off = 0;
+    for (uint32_t s = 0; s < nscenes; ++s) {
+        mp_scene_desc d;
+        if (descs) d = descs[s];
+        else fill_default_desc(d);
+        const uint32_t sid = scene_ids ? scene_ids[s] : MP_SCENE_CUBE_DROP;
+        const int rc = seed_scene(params[s], sid, d, counts[s], tmp);
+        if (rc != MP_OK) return rc;
+        std::copy(tmp.begin(), tmp.end(), pos.begin() + 4 * off);
+        std::fill(scene_of.begin() + off, scene_of.begin() + off + counts[s], s);
+        std::memset(&hs[s], 0, sizeof(SceneDev));
+        hs[s].c = make_consts(params[s], grids[s], counts[s], dts[s], sid == MP_SCENE_SPHERE_DROP);
+        hs[s].p0 = uint32_t(off);
+        for (int a = 0; a < 3; ++a) {
+            hs[s].sphere.c[a] = d.sphere_center[a];
+            hs[s].sphere.v[a] = d.sphere_velocity[a];
+        }
+        hs[s].sphere.r = params[s].sphere_radius;
+        off += counts[s];
+    }
+    DeviceGuard g(b->device);
+    b->free_all();
+    b->S = nscenes;
+    b->N = uint32_t(total);
+    b->iterations = iters;
+    b->counts.assign(counts, counts + nscenes);
+    b->scene_ids.assign(nscenes, MP_SCENE_CUBE_DROP);
+    if (scene_ids) b->scene_ids.assign(scene_ids, scene_ids + nscenes);
+    b->params.assign(params, params + nscenes);
+    b->dts.assign(dts, dts + nscenes);
+    b->p0.resize(nscenes);
+    for (uint32_t s = 0; s < nscenes; ++s) b->p0[s] = hs[s].p0;
+    b->host_scenes = hs;
+    b->max_cells = uint32_t(worst_cells);
+    // particles
+    const uint32_t cap = round_up(std::max<uint32_t>(b->N, 1u), 256u);
+    const size_t v4 = size_t(cap) * 16, u = size_t(cap) * 4;
+    const size_t longs = (size_t(cap) / kSegMax + 2) * 4;
+    const size_t ptotal = 5 * v4 + 19 * u + longs + 32 * 256;
+    MP_CUDA(cudaMalloc(&b->particle_block, ptotal));
+    MP_CUDA(cudaMemset(b->particle_block, 0, ptotal));
+    char* pb = static_cast<char*>(b->particle_block);
+    auto take = [&](size_t bytes) {
+        char* r = pb;
+        pb += (bytes + 255) & ~size_t(255);
+        return r;
+    };
+    BatchArgs& a = b->a;
+    a.pos = reinterpret_cast<float4*>(take(v4));
+    a.vel = reinterpret_cast<float4*>(take(v4));
+    a.prev = reinterpret_cast<float4*>(take(v4));
+    a.sorted_a = reinterpret_cast<float4*>(take(v4));
+    a.sorted_b = reinterpret_cast<float4*>(take(v4));
+    a.hash = reinterpret_cast<uint32_t*>(take(u));
+    a.off = reinterpret_cast<uint32_t*>(take(u));
+    a.tmp = reinterpret_cast<uint32_t*>(take(u));
+    a.sidx = reinterpret_cast<uint32_t*>(take(u));
+    a.scell = reinterpret_cast<uint32_t*>(take(u));
+    a.ncount = reinterpret_cast<uint32_t*>(take(u));
+    a.lambdas = reinterpret_cast<float*>(take(u));
+    a.foam = reinterpret_cast<float*>(take(u));
+    uint32_t* so = reinterpret_cast<uint32_t*>(take(u));
+    a.scene_of = so;
+    a.row_masks = reinterpret_cast<uint32_t*>(take(9 * u));
+    a.mask_overflow = reinterpret_cast<uint32_t*>(take(u));
+    a.mask_stride = cap;
+    a.long_list = reinterpret_cast<uint32_t*>(take(longs));
+    // cells: counts + cstart for the worst case (every scene's whole box)
+    const size_t clen = size_t(b->max_cells) + 1;
+    const size_t tiles = clen / 128 + 2;
+    const size_t cbytes = ((clen * 4 + 255) & ~size_t(255));
+    MP_CUDA(cudaMalloc(&b->cell_block, 2 * cbytes + tiles * 4));
+    MP_CUDA(cudaMemset(b->cell_block, 0, 2 * cbytes + tiles * 4));
+    a.counts = static_cast<uint32_t*>(b->cell_block);
+    a.cstart = reinterpret_cast<uint32_t*>(static_cast<char*>(b->cell_block) + cbytes);
+    a.tile_sums = reinterpret_cast<uint32_t*>(static_cast<char*>(b->cell_block) + 2 * cbytes);
+    a.max_cells = b->max_cells;
+    MP_CUDA(cudaMalloc(&b->small_block, 256));
+    MP_CUDA(cudaMemset(b->small_block, 0, 256));
+    uint32_t* sm = static_cast<uint32_t*>(b->small_block);
+    a.long_count = sm + 0;
+    a.total_cells = sm + 1;
+    a.err = sm + 2;
+    a.bar_count = reinterpret_cast<unsigned*>(sm + 32);
+    a.bar_gen = reinterpret_cast<unsigned*>(sm + 33);
+    MP_CUDA(cudaMalloc(&b->scenes, sizeof(SceneDev) * std::max<uint32_t>(nscenes, 1u)));
+    a.scenes = b->scenes;
+    a.iterations = iters;
+    int rc = b->upload_scenes();
+    if (rc != MP_OK) return rc;
+    if (total) {
+        MP_CUDA(cudaMemcpy(a.pos, pos.data(), 16 * size_t(total), cudaMemcpyHostToDevice));
+        MP_CUDA(cudaMemcpy(so, scene_of.data(), 4 * size_t(total), cudaMemcpyHostToDevice));
+    }
+    // launch shape: the cached autotuning result for this size, if any
+    {
+        std::lock_guard<std::mutex> lock(g_tune_lock);
+        auto it = g_tune_cache.find({pow2_bucket(b->N), b->S});
+        if (it != g_tune_cache.end()) {
+            b->block = it->second.first;
+            b->blocks_per_sm = it->second.second;
+        }
+    }
+    MP_CUDA(cudaDeviceSynchronize());
+    return MP_OK;
+}
+
+int mp_batch_set_dts(mp_batch* b, const float* dts) {
+    if (!b || (b->S && !dts)) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (uint32_t s = 0; s < b->S; ++s) {
+        if (!(dts[s] > 0.0f)) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u: dt must be > 0", s);
+    }
+    DeviceGuard g(b->device);
+    MP_CUDA(cudaDeviceSynchronize());
+    // refresh the constants that depend on dt, keep the device-side sphere state
+    std::vector<SceneDev> cur(b->S);
+    if (b->S) MP_CUDA(cudaMemcpy(cur.data(), b->scenes, sizeof(SceneDev) * b->S, cudaMemcpyDeviceToHost));
+    for (uint32_t s = 0; s < b->S; ++s) {
+        GridDev g0;
+        make_grid(b->params[s], g0);
+        cur[s].c = make_consts(b->params[s], g0, b->counts[s], dts[s],
+                               b->scene_ids[s] == MP_SCENE_SPHERE_DROP);
+        b->dts[s] = dts[s];
+    }
+    if (b->S) MP_CUDA(cudaMemcpy(b->scenes, cur.data(), sizeof(SceneDev) * b->S, cudaMemcpyHostToDevice));
+    b->drop_graph();
+    return MP_OK;
+}
+
+int mp_batch_step(mp_batch* b, mp_stream stream) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    DeviceGuard g(b->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!b->graph_mode) return b->enqueue(s);
+    if (!b->gexec) {
+        if (!b->cap_stream) MP_CUDA(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+        MP_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = b->enqueue(b->cap_stream);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(b->cap_stream, &graph);
+        if (rc != MP_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(MP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        b->graph = graph;
+        MP_CUDA(cudaGraphInstantiate(&b->gexec, b->graph, 0));
+    }
+    MP_CUDA(cudaGraphLaunch(b->gexec, s));
+    return MP_OK;
+}
+
+int mp_batch_set_mode(mp_batch* b, int serial) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    b->serial = serial != 0;
+    b->drop_graph();
+    return MP_OK;
+}
+
+int mp_batch_set_graph_mode(mp_batch* b, int enable) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    DeviceGuard g(b->device);
+    b->graph_mode = enable != 0;
+    b->drop_graph();
+    return MP_OK;
+}
+
+int mp_batch_set_launch(mp_batch* b, uint32_t block, uint32_t blocks_per_sm) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    DeviceGuard g(b->device);
+    const int occ = batch_max_blocks_per_sm(block);
+    if (occ <= 0) return fail(MP_ERR_INVALID_ARGUMENT, "block size %u is not 128, 256 or 512", block);
+    if (blocks_per_sm > uint32_t(occ))
+        return fail(MP_ERR_INVALID_ARGUMENT, "%u blocks/SM exceed the %d that fit", blocks_per_sm, occ);
+    b->block = block;
+    b->blocks_per_sm = blocks_per_sm;
+    b->drop_graph();
+    return MP_OK;
+}
+
+int mp_batch_get_launch(const mp_batch* b, uint32_t* block, uint32_t* blocks) {
+    if (!b || !block || !blocks) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    *block = b->block;
+    *blocks = b->blocks();
+    return MP_OK;
+}
+
+int mp_batch_autotune(mp_batch* b, uint32_t steps, mp_batch_tuning* best) {
+    if (!b || steps == 0) return fail(MP_ERR_INVALID_ARGUMENT, "bad argument");
+    DeviceGuard g(b->device);
+    if (b->N == 0) return MP_OK;
+    // Each candidate runs `steps` steps from the same saved state, which is
+    // restored afterwards: tuning does not advance the simulation.
+    const size_t v4 = size_t(b->N) * 16;
+    void* save = nullptr;
+    MP_CUDA(cudaMalloc(&save, 2 * v4 + sizeof(SceneDev) * b->S));
+    auto snapshot = [&](bool restore) -> int {
+        char* sv = static_cast<char*>(save);
+        const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+        if (restore) {
+            MP_CUDA(cudaMemcpy(b->a.pos, sv, v4, k));
+            MP_CUDA(cudaMemcpy(b->a.vel, sv + v4, v4, k));
+            MP_CUDA(cudaMemcpy(b->scenes, sv + 2 * v4, sizeof(SceneDev) * b->S, k));
+        } else {
+            MP_CUDA(cudaMemcpy(sv, b->a.pos, v4, k));
+            MP_CUDA(cudaMemcpy(sv + v4, b->a.vel, v4, k));
+            MP_CUDA(cudaMemcpy(sv + 2 * v4, b->scenes, sizeof(SceneDev) * b->S, k));
+        }
+        return MP_OK;
+    };
+    int rc = snapshot(false);
+    const uint32_t saved_block = b->block, saved_bps = b->blocks_per_sm;
+    const bool saved_graph = b->graph_mode;
+    b->graph_mode = false;
+    b->drop_graph();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best_ms = 1e30f;
+    uint32_t best_block = saved_block, best_bps = saved_bps;
+    for (uint32_t block : {128u, 256u, 512u}) {
+        const int occ = batch_max_blocks_per_sm(block);
+        for (int bps = 1; rc == MP_OK && bps <= occ; ++bps) {
+            b->block = block;
+            b->blocks_per_sm = uint32_t(bps);
+            rc = snapshot(true);
+            if (rc != MP_OK) break;
+            rc = b->enqueue(nullptr);  // warm-up step
+            cudaEventRecord(e0);
+            for (uint32_t i = 0; rc == MP_OK && i < steps; ++i) rc = b->enqueue(nullptr);
+            cudaEventRecord(e1);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(MP_ERR_CUDA, "autotune sync failed");
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= float(steps);
+            if (rc == MP_OK && ms < best_ms) {
+                best_ms = ms;
+                best_block = block;
+                best_bps = uint32_t(bps);
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int rc2 = snapshot(true);
+    cudaFree(save);
+    b->graph_mode = saved_graph;
+    if (rc != MP_OK || rc2 != MP_OK) {
+        b->block = saved_block;
+        b->blocks_per_sm = saved_bps;
+        return rc != MP_OK ? rc : rc2;
+    }
+    b->block = best_block;
+    b->blocks_per_sm = best_bps;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_lock);
+        g_tune_cache[{pow2_bucket(b->N), b->S}] = {best_block, best_bps};
+    }
+    if (best) {
+        best->block = best_block;
+        best->blocks_per_sm = best_bps;
+        best->ms_per_step = best_ms;
+    }
+    MP_CUDA(cudaDeviceSynchronize());
+    return MP_OK;
+}
+
+uint32_t mp_batch_scene_count(const mp_batch* b) { return b ? b->S : 0; }
+uint32_t mp_batch_particle_count(const mp_batch* b) { return b ? b->N : 0; }
+
+int mp_batch_scene_range(const mp_batch* b, uint32_t scene, uint32_t* first, uint32_t* count) {
+    if (!b || !first || !count) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (scene >= b->S) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u >= %u", scene, b->S);
+    *first = b->p0[scene];
+    *count = b->counts[scene];
+    return MP_OK;
+}
+
+int mp_batch_buffer(mp_batch* b, uint32_t which, void** dptr, size_t* bytes) {
+    return batch_buffer(b, which, dptr, bytes);
+}
+
+int mp_batch_upload(mp_batch* b, uint32_t which, const void* host, size_t count, mp_stream stream) {
+    void* dptr = nullptr;
+    size_t bytes = 0;
+    int rc = batch_buffer(b, which, &dptr, &bytes);
+    if (rc != MP_OK) return rc;
+    const size_t need = count * elem_bytes(which);
+    if (!host && count) return fail(MP_ERR_INVALID_ARGUMENT, "host is NULL");
+    if (need > bytes) return fail(MP_ERR_INVALID_ARGUMENT, "%zu elements exceed buffer %u", count, which);
+    if (!need) return MP_OK;
+    DeviceGuard g(b->device);
+    MP_CUDA(cudaMemcpyAsync(dptr, host, need, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream)));
+    return MP_OK;
+}
+
+int mp_batch_download(mp_batch* b, uint32_t which, void* host, size_t count, mp_stream stream) {
+    void* dptr = nullptr;
+    size_t bytes = 0;
+    int rc = batch_buffer(b, which, &dptr, &bytes);
+    if (rc != MP_OK) return rc;
+    const size_t need = count * elem_bytes(which);
+    if (!host && count) return fail(MP_ERR_INVALID_ARGUMENT, "host is NULL");
+    if (need > bytes) return fail(MP_ERR_INVALID_ARGUMENT, "%zu elements exceed buffer %u", count, which);
+    DeviceGuard g(b->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (need) MP_CUDA(cudaMemcpyAsync(host, dptr, need, cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    return MP_OK;
+}
+
+int mp_batch_set_sphere(mp_batch* b, uint32_t scene, const float center[3], const float velocity[3],
+                        float radius) {
+    if (!b || !center || !velocity) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (scene >= b->S) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u >= %u", scene, b->S);
+    SphereState s{};
+    for (int a = 0; a < 3; ++a) {
+        s.c[a] = center[a];
+        s.v[a] = velocity[a];
+    }
+    s.r = radius;
+    DeviceGuard g(b->device);
+    MP_CUDA(cudaDeviceSynchronize());
+    MP_CUDA(cudaMemcpy(&b->scenes[scene].sphere, &s, sizeof(s), cudaMemcpyHostToDevice));
+    return MP_OK;
+}
+
+int mp_batch_get_sphere(mp_batch* b, uint32_t scene, float center[3], float velocity[3], float* radius) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (scene >= b->S) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u >= %u", scene, b->S);
+    SphereState s{};
+    DeviceGuard g(b->device);
+    MP_CUDA(cudaDeviceSynchronize());
+    MP_CUDA(cudaMemcpy(&s, &b->scenes[scene].sphere, sizeof(s), cudaMemcpyDeviceToHost));
+    for (int a = 0; a < 3; ++a) {
+        if (center) center[a] = s.c[a];
+        if (velocity) velocity[a] = s.v[a];
+    }
+    if (radius) *radius = s.r;
+    return MP_OK;
+}
+
+int mp_batch_check_errors(mp_batch* b, uint32_t* bits) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    DeviceGuard g(b->device);
+    MP_CUDA(cudaDeviceSynchronize());
+    uint32_t w = 0;
+    if (b->a.err) {
+        MP_CUDA(cudaMemcpy(&w, b->a.err, 4, cudaMemcpyDeviceToHost));
+        MP_CUDA(cudaMemset(b->a.err, 0, 4));
+    }
+    if (bits) *bits = w;
+    if (w & kDevErrSpin) return fail(MP_ERR_SPIN_LIMIT, "a bounded device wait gave up (bits 0x%x)", w);
+    if (w) return fail(MP_ERR_DEVICE, "device error word 0x%x", w);
+    return MP_OK;
+}
+
+}  // extern "C"

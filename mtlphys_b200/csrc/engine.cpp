@@ -20,19 +20,23 @@
 #include <string>
 #include <vector>
 
+#include "host_common.h"
 #include "pbf_kernels.h"
 
+using namespace mpb;
 using mpb::DevState;
 using mpb::GridDev;
 using mpb::StepConsts;
 
-namespace {
+namespace mpb {
 
 constexpr uint32_t kAbiVersion = 1;
 constexpr float kPi = 3.14159265358979323846f;
 constexpr uint32_t kPad = 256;  // Engine.cpp:19 pads buffers to the threadgroup size
 
+namespace {
 thread_local std::string g_err;
+}  // namespace
 
 int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -44,27 +48,11 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define MP_CUDA(call)                                                                     \
-    do {                                                                                  \
-        const cudaError_t e_ = (call);                                                    \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(e_ == cudaErrorMemoryAllocation ? MP_ERR_OUT_OF_MEMORY : MP_ERR_CUDA, \
-                        "%s: %s", #call, cudaGetErrorString(e_));                         \
-    } while (0)
+// Lets the other translation units of the library report through
+// mp_last_error().
+void record_error(const char* msg) { g_err = msg; }
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
-
-uint32_t round_up(uint32_t n, uint32_t m) { return ((n + m - 1) / m) * m; }
+const char* last_error() { return g_err.c_str(); }
 
 // Grid of buildSpatialBuffers (Engine.cpp:398-403, 443-451).
 int make_grid(const mp_pbf_params& p, GridDev& g) {
@@ -259,6 +247,59 @@ size_t elem_bytes(uint32_t which) {
     }
 }
 
+// writePBFParams (Engine.cpp:551-572) and the shader literals, in FP32 like
+// the reference, for a scene of n particles on grid g stepped by dt.
+StepConsts make_consts(const mp_pbf_params& p, const GridDev& g, uint32_t n, float dt, bool sphere) {
+    StepConsts c{};
+    c.g = g;
+    c.n = n;
+    const float h = p.h, h2 = h * h, h3 = h2 * h, h6 = h3 * h3, h9 = h6 * h3;
+    c.h = h;
+    c.h2 = h2;
+    c.poly6 = 315.0f / (64.0f * kPi * h9);
+    c.spiky = 45.0f / (kPi * h6);
+    c.inv_rho0 = 1.0f / p.rest_density;
+    c.eps = p.epsilon;
+    c.scorr_k = p.scorr_k;
+    c.scorr_n = p.scorr_n;
+    // invWq = 1 / poly6((dq*h)^2) (Constraints.metal:159-160)
+    const float dq = p.scorr_dq * h;
+    const float dq2 = dq * dq;
+    const float wd = h2 - dq2;
+    const float wq = dq2 < h2 ? c.poly6 * wd * wd * wd : 0.0f;
+    c.inv_wq = wq > 0.0f ? 1.0f / wq : 0.0f;
+    c.max_step = p.max_delta * h;
+    c.bminx = p.bounds_min[0];
+    c.bminy = p.bounds_min[1];
+    c.bminz = p.bounds_min[2];
+    c.bmaxx = p.bounds_max[0];
+    c.bmaxy = p.bounds_max[1];
+    c.bmaxz = p.bounds_max[2];
+    c.gravx = p.gravity[0];
+    c.gravy = p.gravity[1];
+    c.gravz = p.gravity[2];
+    c.dt = dt;
+    c.inv_dt = 1.0f / dt;
+    c.damping = p.damping;
+    c.vmax = p.vmax * h * c.inv_dt;
+    c.vmax_frac = p.vmax;
+    c.wall_eps = p.wall_eps;
+    c.floor_fric = p.floor_friction;
+    c.wall_fric = p.wall_friction;
+    c.foam_maxn = p.foam_max_neighbors;
+    c.foam_lo = p.foam_speed_lo;
+    c.foam_hi = p.foam_speed_hi;
+    c.sphere = sphere ? 1 : 0;
+    c.sph_gravity = p.sphere_gravity;
+    c.sph_drag = p.sphere_drag;
+    c.sph_rest = p.sphere_restitution;
+    return c;
+}
+
+}  // namespace mpb
+
+namespace {
+
 // Per-kernel CUDA-event timing (mp_engine_set_profiling): two events per
 // launch on the launching stream, reduced to totals per kernel name when read.
 struct EventTimer final : mpb::KernelTimer {
@@ -436,52 +477,7 @@ struct mp_engine {
     }
 
     StepConsts consts(float dt) const {
-        const mp_pbf_params& p = params;
-        StepConsts c{};
-        c.g = grid;
-        c.n = n;
-        // writePBFParams (Engine.cpp:551-572), in FP32 like the reference.
-        const float h = p.h, h2 = h * h, h3 = h2 * h, h6 = h3 * h3, h9 = h6 * h3;
-        c.h = h;
-        c.h2 = h2;
-        c.poly6 = 315.0f / (64.0f * kPi * h9);
-        c.spiky = 45.0f / (kPi * h6);
-        c.inv_rho0 = 1.0f / p.rest_density;
-        c.eps = p.epsilon;
-        c.scorr_k = p.scorr_k;
-        c.scorr_n = p.scorr_n;
-        // invWq = 1 / poly6((dq*h)^2) (Constraints.metal:159-160)
-        const float dq = p.scorr_dq * h;
-        const float dq2 = dq * dq;
-        const float wd = h2 - dq2;
-        const float wq = dq2 < h2 ? c.poly6 * wd * wd * wd : 0.0f;
-        c.inv_wq = wq > 0.0f ? 1.0f / wq : 0.0f;
-        c.max_step = p.max_delta * h;
-        c.bminx = p.bounds_min[0];
-        c.bminy = p.bounds_min[1];
-        c.bminz = p.bounds_min[2];
-        c.bmaxx = p.bounds_max[0];
-        c.bmaxy = p.bounds_max[1];
-        c.bmaxz = p.bounds_max[2];
-        c.gravx = p.gravity[0];
-        c.gravy = p.gravity[1];
-        c.gravz = p.gravity[2];
-        c.dt = dt;
-        c.inv_dt = 1.0f / dt;
-        c.damping = p.damping;
-        c.vmax = p.vmax * h * c.inv_dt;
-        c.vmax_frac = p.vmax;
-        c.wall_eps = p.wall_eps;
-        c.floor_fric = p.floor_friction;
-        c.wall_fric = p.wall_friction;
-        c.foam_maxn = p.foam_max_neighbors;
-        c.foam_lo = p.foam_speed_lo;
-        c.foam_hi = p.foam_speed_hi;
-        c.sphere = scene == MP_SCENE_SPHERE_DROP ? 1 : 0;
-        c.sph_gravity = p.sphere_gravity;
-        c.sph_drag = p.sphere_drag;
-        c.sph_rest = p.sphere_restitution;
-        return c;
+        return mpb::make_consts(params, grid, n, dt, scene == MP_SCENE_SPHERE_DROP);
     }
 
     int enqueue_step(float dt, cudaStream_t s, mpb::KernelTimer* t = nullptr) {
@@ -495,13 +491,9 @@ struct mp_engine {
 
 extern "C" {
 
-const char* mp_last_error(void) { return g_err.c_str(); }
+const char* mp_last_error(void) { return mpb::last_error(); }
 
 }  // extern "C"
-
-// Lets the other translation units of the library report through
-// mp_last_error().
-void mpb::record_error(const char* msg) { g_err = msg; }
 
 extern "C" {
 
