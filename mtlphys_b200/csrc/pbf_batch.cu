@@ -210,7 +210,9 @@ __global__ void __launch_bounds__(BS) k_batch_step(BatchArgs a) {
     }
     grid_barrier(a.bar_count, a.bar_gen, a.err);
     if (blockIdx.x == 0) {
-        uint32_t running = 0;
+        // slots of this launch start at its first particle (a scene's range
+        // in serial mode)
+        uint32_t running = pb;
         for (uint32_t t0 = 0; t0 < tiles; t0 += BS) {
             const uint32_t t = t0 + threadIdx.x;
             const uint32_t v = t < tiles ? a.tile_sums[t] : 0u;

@@ -135,9 +135,9 @@ __device__ __forceinline__ float pow_n(float x, uint32_t n) {
 }
 
 __device__ __forceinline__ float smoothstep_f(float e0, float e1, float x) {
-    float t = (x - e0) / (e1 - e0);
+    float t = __fdiv_rn(__fsub_rn(x, e0), __fsub_rn(e1, e0));
     t = fminf(fmaxf(t, 0.0f), 1.0f);
-    return t * t * (3.0f - 2.0f * t);
+    return __fmul_rn(__fmul_rn(t, t), __fmaf_rn(-2.0f, t, 3.0f));
 }
 
 #endif  // __CUDACC__

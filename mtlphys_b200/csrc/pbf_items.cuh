@@ -219,43 +219,61 @@ struct RowMasks {
     uint32_t stride;
 };
 
+// The solver arithmetic below is written with explicit round-to-nearest
+// operations (__fmaf_rn, __fmul_rn, __fadd_rn, and their FP64 forms): the
+// compiler may not fuse or split them, so every kernel that inlines these
+// functions (the single-scene kernels, the persistent batch kernel) rounds
+// identically and gives bit-identical results.
+
 // Density / gradient terms of one in-range candidate at offset r, r2 = |r|^2
 // < h^2 (Constraints.metal:112-118).  The particle itself (r2 = 0) adds W(0).
 struct LambdaAcc {
     float dens = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f, gsq = 0.0f;
     __device__ __forceinline__ void add(const StepConsts& c, float rx, float ry, float rz, float r2) {
-        const float d = c.h2 - r2;
-        dens += c.poly6 * d * d * d;
+        const float d = __fsub_rn(c.h2, r2);
+        dens = __fmaf_rn(__fmul_rn(__fmul_rn(c.poly6, d), d), d, dens);
         if (r2 > 1e-12f) {
             const float rinv = rsqrtf(r2);
-            const float hd = fmaxf(c.h - r2 * rinv, 0.0f);
-            const float sc = -c.spiky * hd * hd * rinv;
-            gx += sc * rx;
-            gy += sc * ry;
-            gz += sc * rz;
-            gsq += sc * sc * r2;
+            const float hd = fmaxf(__fsub_rn(c.h, __fmul_rn(r2, rinv)), 0.0f);
+            const float sc = __fmul_rn(__fmul_rn(__fmul_rn(-c.spiky, hd), hd), rinv);
+            gx = __fmaf_rn(sc, rx, gx);
+            gy = __fmaf_rn(sc, ry, gy);
+            gz = __fmaf_rn(sc, rz, gz);
+            gsq = __fmaf_rn(__fmul_rn(sc, sc), r2, gsq);
         }
     }
     __device__ __forceinline__ float lambda(const StepConsts& c) const {
-        const float C = dens * c.inv_rho0 - 1.0f;
-        const float denom = c.inv_rho0 * c.inv_rho0 * (gx * gx + gy * gy + gz * gz + gsq) + c.eps;
-        return -C / denom;
+        const float C = __fmaf_rn(dens, c.inv_rho0, -1.0f);
+        const float g2 = __fmaf_rn(gz, gz, __fmaf_rn(gy, gy, __fmaf_rn(gx, gx, gsq)));
+        const float denom = __fmaf_rn(__fmul_rn(c.inv_rho0, c.inv_rho0), g2, c.eps);
+        return __fdiv_rn(-C, denom);
     }
 };
+
+__device__ __forceinline__ float pow_n_rn(float x, uint32_t n) {
+    if (n == 4u) {
+        const float x2 = __fmul_rn(x, x);
+        return __fmul_rn(x2, x2);
+    }
+    float r = 1.0f;
+    for (uint32_t e = 0; e < n; ++e) r = __fmul_rn(r, x);
+    return r;
+}
 
 // Position-correction term of one in-range candidate (Constraints.metal:170-181).
 __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float lj, float rx, float ry,
                                           float rz, float r2, float& dx, float& dy, float& dz) {
     if (r2 > 1e-12f) {
-        const float d = c.h2 - r2;
-        const float ratio = c.poly6 * d * d * d * c.inv_wq;
-        const float scorr = -c.scorr_k * pow_n(ratio, c.scorr_n);
+        const float d = __fsub_rn(c.h2, r2);
+        const float ratio = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(c.poly6, d), d), d), c.inv_wq);
+        const float scorr = __fmul_rn(-c.scorr_k, pow_n_rn(ratio, c.scorr_n));
         const float rinv = rsqrtf(r2);
-        const float hd = fmaxf(c.h - r2 * rinv, 0.0f);
-        const float coef = (li + lj + scorr) * (-c.spiky * hd * hd * rinv);
-        dx += coef * rx;
-        dy += coef * ry;
-        dz += coef * rz;
+        const float hd = fmaxf(__fsub_rn(c.h, __fmul_rn(r2, rinv)), 0.0f);
+        const float coef = __fmul_rn(__fadd_rn(__fadd_rn(li, lj), scorr),
+                                     __fmul_rn(__fmul_rn(__fmul_rn(-c.spiky, hd), hd), rinv));
+        dx = __fmaf_rn(coef, rx, dx);
+        dy = __fmaf_rn(coef, ry, dy);
+        dz = __fmaf_rn(coef, rz, dz);
     }
 }
 
@@ -300,14 +318,14 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
         const float aix = anchor_x(c.g, pcx);
         aiy = anchor_y(c.g, pcy);
         aiz = anchor_z(c.g, pcz);
-        ox0 = (aix - anchor_x(c.g, x0)) + px;
-        ox1 = (aix - anchor_x(c.g, x0 + 1)) + px;
-        ox2 = (aix - anchor_x(c.g, x0 + 2)) + px;
+        ox0 = __fadd_rn(__fsub_rn(aix, anchor_x(c.g, x0)), px);
+        ox1 = __fadd_rn(__fsub_rn(aix, anchor_x(c.g, x0 + 1)), px);
+        ox2 = __fadd_rn(__fsub_rn(aix, anchor_x(c.g, x0 + 2)), px);
     }
     for (int z = z0; z <= z1; ++z) {
-        const float oz = ANCHORED ? (aiz - anchor_z(c.g, z)) + pz : pz;
+        const float oz = ANCHORED ? __fadd_rn(__fsub_rn(aiz, anchor_z(c.g, z)), pz) : pz;
         for (int y = y0; y <= y1; ++y) {
-            const float oy = ANCHORED ? (aiy - anchor_y(c.g, y)) + py : py;
+            const float oy = ANCHORED ? __fadd_rn(__fsub_rn(aiy, anchor_y(c.g, y)), py) : py;
             const uint32_t base = cell_hash(c.g, x0, y, z);
             const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
             const uint32_t b2 = nx > 1 ? cstart[base + 2] : b1;
@@ -319,7 +337,7 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
                 for (uint32_t k = c0; k < c1; ++k) {
                     const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
                     const float4 q = __ldg(&src[k]);
-                    const float r2 = dist2(ox - q.x, oy - q.y, oz - q.z);
+                    const float r2 = dist2(__fsub_rn(ox, q.x), __fsub_rn(oy, q.y), __fsub_rn(oz, q.z));
                     mask |= uint32_t(r2 < c.h2) << (k - c0);
                 }
                 if (c0 == b0) first = mask;
@@ -329,7 +347,7 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
                     mask &= mask - 1;
                     const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
                     const float4 q = __ldg(&src[k]);
-                    const float rx = ox - q.x, ry = oy - q.y, rz = oz - q.z;
+                    const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y), rz = __fsub_rn(oz, q.z);
                     body(q, rx, ry, rz, dist2(rx, ry, rz));
                 }
             }
@@ -373,8 +391,8 @@ __device__ __forceinline__ void lambda_first_item(const StepConsts& c, uint32_t 
     const float lambda = acc.lambda(c);
     // l = p - A(c): exact for the particle's own cell (Sterbenz), so the
     // anchored state starts equal to the FP32 predicted position.
-    nxt[s] = make_float4(p.x - anchor_x(c.g, cx), p.y - anchor_y(c.g, cy), p.z - anchor_z(c.g, cz),
-                         lambda);
+    nxt[s] = make_float4(__fsub_rn(p.x, anchor_x(c.g, cx)), __fsub_rn(p.y, anchor_y(c.g, cy)),
+                         __fsub_rn(p.z, anchor_z(c.g, cz)), lambda);
     scell[s] = cell_local(c.g, cx, cy, cz);
     const uint32_t j = sidx[s];
     // the particle itself was counted iff its own distance test passed
@@ -395,8 +413,8 @@ __device__ __forceinline__ void lambda_item(const StepConsts& c, uint32_t s,
     const float4 l = cur[s];
     int pcx, pcy, pcz, cx, cy, cz;
     decode_cell(c.g, scell[s], pcx, pcy, pcz);
-    cell_of(c.g, anchor_x(c.g, pcx) + l.x, anchor_y(c.g, pcy) + l.y, anchor_z(c.g, pcz) + l.z, cx,
-            cy, cz);
+    cell_of(c.g, __fadd_rn(anchor_x(c.g, pcx), l.x), __fadd_rn(anchor_y(c.g, pcy), l.y),
+            __fadd_rn(anchor_z(c.g, pcz), l.z), cx, cy, cz);
     LambdaAcc acc;
     sweep<true>(c, cur, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s, rm.rows ? &rm : nullptr,
                 [&](const float4&, float rx, float ry, float rz, float r2) { acc.add(c, rx, ry, rz, r2); });
@@ -419,12 +437,14 @@ __device__ __forceinline__ void finalize_particle(const StepConsts& c, uint32_t 
     Y = fmin(fmax(Y, by0), by1);
     Z = fmin(fmax(Z, bz0), bz1);
     const float4 pr = prev[j];
-    const double k = (1.0 / double(c.dt)) * double(c.damping);
-    double vx = (X - double(pr.x)) * k, vy = (Y - double(pr.y)) * k, vz = (Z - double(pr.z)) * k;
+    const double k = __dmul_rn(__drcp_rn(double(c.dt)), double(c.damping));
+    double vx = __dmul_rn(__dsub_rn(X, double(pr.x)), k);
+    double vy = __dmul_rn(__dsub_rn(Y, double(pr.y)), k);
+    double vz = __dmul_rn(__dsub_rn(Z, double(pr.z)), k);
     const double we = c.wall_eps;
-    const bool xMin = X <= bx0 + we, xMax = X >= bx1 - we;
-    const bool yMin = Y <= by0 + we, yMax = Y >= by1 - we;
-    const bool zMin = Z <= bz0 + we, zMax = Z >= bz1 - we;
+    const bool xMin = X <= __dadd_rn(bx0, we), xMax = X >= __dsub_rn(bx1, we);
+    const bool yMin = Y <= __dadd_rn(by0, we), yMax = Y >= __dsub_rn(by1, we);
+    const bool zMin = Z <= __dadd_rn(bz0, we), zMax = Z >= __dsub_rn(bz1, we);
     if (xMin) vx = fmax(vx, 0.0);
     if (xMax) vx = fmin(vx, 0.0);
     if (yMin) vy = fmax(vy, 0.0);
@@ -432,26 +452,26 @@ __device__ __forceinline__ void finalize_particle(const StepConsts& c, uint32_t 
     if (zMin) vz = fmax(vz, 0.0);
     if (zMax) vz = fmin(vz, 0.0);
     if (yMin) {
-        vx *= double(c.floor_fric);
-        vz *= double(c.floor_fric);
+        vx = __dmul_rn(vx, double(c.floor_fric));
+        vz = __dmul_rn(vz, double(c.floor_fric));
     } else if (xMin || xMax || zMin || zMax) {
-        vx *= double(c.wall_fric);
-        vy *= double(c.wall_fric);
-        vz *= double(c.wall_fric);
+        vx = __dmul_rn(vx, double(c.wall_fric));
+        vy = __dmul_rn(vy, double(c.wall_fric));
+        vz = __dmul_rn(vz, double(c.wall_fric));
     }
-    const double vmax = double(c.vmax_frac) * double(c.h) / double(c.dt);
-    double vl = sqrt(vx * vx + vy * vy + vz * vz);
+    const double vmax = __ddiv_rn(__dmul_rn(double(c.vmax_frac), double(c.h)), double(c.dt));
+    double vl = __dsqrt_rn(__fma_rn(vz, vz, __fma_rn(vy, vy, __dmul_rn(vx, vx))));
     if (vl > vmax) {
-        const double f = vmax / vl;
-        vx *= f;
-        vy *= f;
-        vz *= f;
-        vl = sqrt(vx * vx + vy * vy + vz * vz);
+        const double f = __ddiv_rn(vmax, vl);
+        vx = __dmul_rn(vx, f);
+        vy = __dmul_rn(vy, f);
+        vz = __dmul_rn(vz, f);
+        vl = __dsqrt_rn(__fma_rn(vz, vz, __fma_rn(vy, vy, __dmul_rn(vx, vx))));
     }
     pos[j] = make_float4(float(X), float(Y), float(Z), 1.0f);
     vel[j] = make_float4(float(vx), float(vy), float(vz), 0.0f);
-    const float surface = 1.0f - fminf(fmaxf(float(ncount[j]) / c.foam_maxn, 0.0f), 1.0f);
-    foam[j] = surface * smoothstep_f(c.foam_lo, c.foam_hi, float(vl));
+    const float surface = __fsub_rn(1.0f, fminf(fmaxf(__fdiv_rn(float(ncount[j]), c.foam_maxn), 0.0f), 1.0f));
+    foam[j] = __fmul_rn(surface, smoothstep_f(c.foam_lo, c.foam_hi, float(vl)));
     if (!(isfinite(X + Y + Z) && isfinite(vx + vy + vz))) atomicOr(err, kDevErrNaN);
 }
 
@@ -474,7 +494,7 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
     decode_cell(c.g, scell[s], pcx, pcy, pcz);
     const float ax = anchor_x(c.g, pcx), ay = anchor_y(c.g, pcy), az = anchor_z(c.g, pcz);
     int cx, cy, cz;
-    cell_of(c.g, ax + l.x, ay + l.y, az + l.z, cx, cy, cz);
+    cell_of(c.g, __fadd_rn(ax, l.x), __fadd_rn(ay, l.y), __fadd_rn(az, l.z), cx, cy, cz);
     float dx = 0.0f, dy = 0.0f, dz = 0.0f;
     auto body = [&](const float4& q, float rx, float ry, float rz, float r2) {
         delta_add(c, l.w, q.w, rx, ry, rz, r2, dx, dy, dz);
@@ -486,15 +506,15 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
         const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
         const int nx = x1 - x0 + 1;
         if (nx > 0) {
-            const float ox0 = (ax - anchor_x(c.g, x0)) + l.x;
-            const float ox1 = (ax - anchor_x(c.g, x0 + 1)) + l.x;
-            const float ox2 = (ax - anchor_x(c.g, x0 + 2)) + l.x;
+            const float ox0 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0)), l.x);
+            const float ox1 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 1)), l.x);
+            const float ox2 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 2)), l.x);
             for (int z = z0; z <= z1; ++z) {
-                const float oz = (az - anchor_z(c.g, z)) + l.z;
+                const float oz = __fadd_rn(__fsub_rn(az, anchor_z(c.g, z)), l.z);
                 for (int y = y0; y <= y1; ++y) {
                     uint32_t mask = rm.rows[uint32_t((z - z0) * 3 + (y - y0)) * rm.stride + s];
                     if (mask == 0u) continue;
-                    const float oy = (ay - anchor_y(c.g, y)) + l.y;
+                    const float oy = __fadd_rn(__fsub_rn(ay, anchor_y(c.g, y)), l.y);
                     const uint32_t base = cell_hash(c.g, x0, y, z);
                     const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
                     const uint32_t b2 = nx > 1 ? cstart[base + 2] : b1;
@@ -503,7 +523,8 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
                         mask &= mask - 1;
                         const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
                         const float4 q = __ldg(&src[k]);
-                        const float rx = ox - q.x, ry = oy - q.y, rz = oz - q.z;
+                        const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y);
+                        const float rz = __fsub_rn(oz, q.z);
                         body(q, rx, ry, rz, dist2(rx, ry, rz));
                     }
                 }
@@ -513,36 +534,37 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
         sweep<true>(c, src, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s,
                     static_cast<const RowMasks*>(nullptr), body);
     }
-    dx *= c.inv_rho0;
-    dy *= c.inv_rho0;
-    dz *= c.inv_rho0;
-    const float dl = sqrtf(dx * dx + dy * dy + dz * dz);
+    dx = __fmul_rn(dx, c.inv_rho0);
+    dy = __fmul_rn(dy, c.inv_rho0);
+    dz = __fmul_rn(dz, c.inv_rho0);
+    const float dl = __fsqrt_rn(dist2(dx, dy, dz));
     if (dl > c.max_step) {
-        const float f = c.max_step / dl;
-        dx *= f;
-        dy *= f;
-        dz *= f;
+        const float f = __fdiv_rn(c.max_step, dl);
+        dx = __fmul_rn(dx, f);
+        dy = __fmul_rn(dy, f);
+        dz = __fmul_rn(dz, f);
     }
     // new position A + (l + delta), box clamp (and sphere push) in FP64
-    double X = double(ax) + double(l.x + dx);
-    double Y = double(ay) + double(l.y + dy);
-    double Z = double(az) + double(l.z + dz);
+    double X = __dadd_rn(double(ax), double(__fadd_rn(l.x, dx)));
+    double Y = __dadd_rn(double(ay), double(__fadd_rn(l.y, dy)));
+    double Z = __dadd_rn(double(az), double(__fadd_rn(l.z, dz)));
     X = fmin(fmax(X, double(c.bminx)), double(c.bmaxx));
     Y = fmin(fmax(Y, double(c.bminy)), double(c.bmaxy));
     Z = fmin(fmax(Z, double(c.bminz)), double(c.bmaxz));
     if (c.sphere) {
         const double scx = sphere->c[0], scy = sphere->c[1], scz = sphere->c[2], sr = sphere->r;
-        const double ex = X - scx, ey = Y - scy, ez = Z - scz;
-        const double e2 = ex * ex + ey * ey + ez * ez;
-        if (e2 < sr * sr) {
-            const double inv = sr / sqrt(fmax(e2, double(1e-8f)));
-            X = scx + ex * inv;
-            Y = scy + ey * inv;
-            Z = scz + ez * inv;
+        const double ex = __dsub_rn(X, scx), ey = __dsub_rn(Y, scy), ez = __dsub_rn(Z, scz);
+        const double e2 = __fma_rn(ez, ez, __fma_rn(ey, ey, __dmul_rn(ex, ex)));
+        if (e2 < __dmul_rn(sr, sr)) {
+            const double inv = __ddiv_rn(sr, __dsqrt_rn(fmax(e2, double(1e-8f))));
+            X = __fma_rn(ex, inv, scx);
+            Y = __fma_rn(ey, inv, scy);
+            Z = __fma_rn(ez, inv, scz);
         }
     }
     if (!LAST) {
-        dst[s] = make_float4(float(X - double(ax)), float(Y - double(ay)), float(Z - double(az)), 0.0f);
+        dst[s] = make_float4(float(__dsub_rn(X, double(ax))), float(__dsub_rn(Y, double(ay))),
+                             float(__dsub_rn(Z, double(az))), 0.0f);
         return;
     }
     finalize_particle(c, sidx[s], X, Y, Z, pos, vel, prev, ncount, foam, err);
