@@ -298,6 +298,8 @@ def run_ours(args, world, rank, local) -> dict | None:
     e2e_value = e2e_ms / (e2e_steps * world)
     e.close()
 
+    batched = None if args.no_batch else run_batched(args, world, rank, local, stream, flush_l2)
+
     if rank != 0:
         return None
     line = {
@@ -317,9 +319,70 @@ def run_ours(args, world, rank, local) -> dict | None:
         "gpu_launches": int(lib.mp_step_launch_count(k_it)) * args.steps,
         "clocks": clk.summary(),
     }
+    if batched is not None:
+        line["batched"] = batched
+        line["gpu_launches"] += batched["launches_timed"]
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args)
     return line
+
+
+def run_batched(args, world, rank, local, stream, flush_l2) -> dict:
+    """The batched ensemble (256 cube drops, 2,000-64,000 particles each,
+    log-uniform): scenes x steps / s with every scene advanced by one
+    persistent launch per step (CUDA graph, autotuned launch shape) against
+    the same kernel launched scene by scene (CUDA graph, its own autotuned
+    shape), from the same start state; the two final states must be
+    bit-identical.  With N ranks the scenes are bin-packed over the ranks by
+    particle count and the time is the max over ranks."""
+    import numpy as np
+    import torch
+
+    from mtlphys_b200 import configs
+    from mtlphys_b200.batch import Batch
+    from mtlphys_b200.ensemble import shard_workload
+
+    full = configs.batch_cubes()
+    w, _ = shard_workload(full, rank, world)
+    steps = max(3, min(args.steps, args.batch_steps))
+    b = Batch(local)
+    res, finals = {}, {}
+    for mode in ("batched", "serial"):
+        b.reset(w.counts, w.params, w.dts, w.scenes, w.descs)
+        b.set_serial(mode == "serial")
+        b.set_graph_mode(False)
+        tune = b.autotune(steps=2)
+        b.set_graph_mode(True)
+        for _ in range(args.warmup):
+            b.step(stream)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush_l2()
+            starts[i].record(stream)
+            b.step(stream)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        if b.check_errors():
+            raise RuntimeError(f"device error in the {mode} batch run")
+        ms = dist_max(sum(s.elapsed_time(t) for s, t in zip(starts, ends)) / steps, world)
+        finals[mode] = (b.positions(), b.velocities())
+        launches = 1 if mode == "batched" else sum(1 for c in w.counts if c > 0)
+        res[mode] = {"ms_per_step": round(ms, 4),
+                     "scenes_per_s": round(len(full.counts) * 1000.0 / ms, 1),
+                     "launch": {"block": tune["block"], "blocks_per_sm": tune["blocks_per_sm"]},
+                     "launches_per_step": launches}
+    b.close()
+    same = all(np.array_equal(x, y) for x, y in zip(finals["batched"], finals["serial"]))
+    return {"workload": full.describe(), "steps": steps, "warmup": args.warmup,
+            "batched": res["batched"], "serial": res["serial"],
+            "speedup": round(res["serial"]["ms_per_step"] / res["batched"]["ms_per_step"], 3),
+            "bit_identical": bool(dist_max(0.0 if same else 1.0, world) == 0.0),
+            "l2": "flushed between timed steps", "mode": "CUDA graph replay",
+            "launches_timed": steps * (res["batched"]["launches_per_step"] + res["serial"]["launches_per_step"])}
 
 
 def read_traffic(kernel: str):
@@ -421,6 +484,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")

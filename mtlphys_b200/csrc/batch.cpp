@@ -101,14 +101,18 @@ struct mp_batch {
             if (e != cudaSuccess) return fail(MP_ERR_CUDA, "batch step launch: %s", cudaGetErrorString(e));
             return MP_OK;
         }
-        for (uint32_t sc = 0; sc < S; ++sc) {  // the same kernel, one scene per launch
+        // The same kernel, one scene per launch, each on a grid no larger
+        // than its particles need (a small scene's grid barriers are cheaper
+        // on fewer blocks; the results do not depend on the grid).
+        for (uint32_t sc = 0; sc < S; ++sc) {
             if (counts[sc] == 0) continue;
+            const uint32_t need = uint32_t((uint64_t(counts[sc]) + block - 1) / block);
             BatchArgs args = a;
             args.scene_begin = sc;
             args.scene_end = sc + 1;
             args.p_begin = p0[sc];
             args.p_end = p0[sc] + counts[sc];
-            const cudaError_t e = launch_batch_step(args, block, nb, s);
+            const cudaError_t e = launch_batch_step(args, block, std::min(nb, need), s);
             if (e != cudaSuccess) return fail(MP_ERR_CUDA, "batch step launch: %s", cudaGetErrorString(e));
         }
         return MP_OK;
