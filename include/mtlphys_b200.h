@@ -254,7 +254,42 @@ int mp_batch_download(mp_batch* b, uint32_t which, void* host, size_t count, mp_
 int mp_batch_set_sphere(mp_batch* b, uint32_t scene, const float center[3], const float velocity[3],
                         float radius);
 int mp_batch_get_sphere(mp_batch* b, uint32_t scene, float center[3], float velocity[3], float* radius);
+/* Replace scene `scene`'s parameters; the box, cell size and
+ * solver_iterations must stay the same (the hash grid does not change). */
+int mp_batch_set_params(mp_batch* b, uint32_t scene, const mp_pbf_params* params);
+int mp_batch_get_params(const mp_batch* b, uint32_t scene, mp_pbf_params* params);
 int mp_batch_check_errors(mp_batch* b, uint32_t* bits);
+
+/* ---- differentiable rollouts (no reference counterpart: the reference
+ *      engine is not differentiable) ------------------------------------------
+ * mp_batch_rollout_forward advances every scene `steps` steps (as
+ * mp_batch_step would) and keeps a checkpoint of the state (positions,
+ * velocities, spheres) every `checkpoint_every` steps.
+ * mp_batch_rollout_backward then takes dL/d(final positions) and dL/d(final
+ * velocities) (device arrays of N float4, w ignored; NULL = zero) and writes
+ * dL/d(initial positions), dL/d(initial velocities) (N float4) and, per scene,
+ * MP_SCENE_GRADS doubles (MP_GRAD_*): dL/d s_corr k and dL/d the initial
+ * sphere center, velocity and radius.  It recomputes each segment between
+ * checkpoints with every step recorded (neighbour lists, iterates,
+ * corrections) and runs the adjoint kernels over it in reverse, the
+ * neighbour topology and clamp states of each step held fixed.  Outputs may
+ * be NULL.  The state is left at the end of the rollout; the scratch buffers
+ * (MP_BUF_PREV, cell and sort arrays, lambdas) then hold values of the
+ * recomputation.  All work is asynchronous on `stream`.  Any other call that
+ * changes the state (step, upload, set_sphere, set_params, set_dts, reset)
+ * ends the rollout: a later backward call fails with MP_ERR_INVALID_ARGUMENT.
+ * Hash grids must be at most 2048 x 2048 x 1024 cells (MP_ERR_UNSUPPORTED). */
+#define MP_SCENE_GRADS   8
+#define MP_GRAD_SCORR_K  0
+#define MP_GRAD_CENTER   1 /* 3 values */
+#define MP_GRAD_VELOCITY 4 /* 3 values */
+#define MP_GRAD_RADIUS   7
+int mp_batch_rollout_forward(mp_batch* b, uint32_t steps, uint32_t checkpoint_every, mp_stream stream);
+int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel, float* dpos0,
+                              float* dvel0, double* dscene, mp_stream stream);
+/* Kernel launches of a backward pass over `steps` steps (recomputation
+ * included). */
+uint32_t mp_batch_rollout_launch_count(const mp_batch* b, uint32_t steps);
 
 /* ---- scan: Engine.hpp:92-100 --------------------------------------------- */
 /* runExclusiveScan(cmd, in, out, chunkSums, n) (Engine.cpp:843-882): out[i]

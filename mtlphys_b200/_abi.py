@@ -25,6 +25,12 @@ MP_SCENE_CUBE_DROP = 0
 MP_SCENE_DAM_BREAK = 1
 MP_SCENE_SPHERE_DROP = 2
 
+MP_SCENE_GRADS = 8
+MP_GRAD_SCORR_K = 0
+MP_GRAD_CENTER = 1
+MP_GRAD_VELOCITY = 4
+MP_GRAD_RADIUS = 7
+
 MP_BUF_POSITIONS = 0
 MP_BUF_VELOCITIES = 1
 MP_BUF_PREV_POSITIONS = 2
@@ -185,6 +191,11 @@ PROTOTYPES = {
     "mp_batch_get_sphere": (_INT, [_VP, _U32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                    C.POINTER(C.c_float)]),
     "mp_batch_check_errors": (_INT, [_VP, C.POINTER(_U32)]),
+    "mp_batch_set_params": (_INT, [_VP, _U32, C.POINTER(PBFParams)]),
+    "mp_batch_get_params": (_INT, [_VP, _U32, C.POINTER(PBFParams)]),
+    "mp_batch_rollout_forward": (_INT, [_VP, _U32, _U32, _VP]),
+    "mp_batch_rollout_backward": (_INT, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "mp_batch_rollout_launch_count": (_U32, [_VP, _U32]),
     "mp_exclusive_scan_scratch_bytes": (_SZ, [_U32]),
     "mp_exclusive_scan": (_INT, [_VP, _VP, _U32, _VP, _SZ, _VP]),
     "mp_exclusive_scan_noalloc": (_INT, [_VP, _VP, _U32, _VP]),

@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import BUF_LAYOUT, MP_BUF_POSITIONS, MP_BUF_VELOCITIES, PBFParams, SceneDesc, check
-from .engine import stream_handle
+from .engine import _CudaArray, stream_handle
 
 
 class Batch:
@@ -129,3 +129,61 @@ class Batch:
         bits = C.c_uint32()
         check(self._lib.mp_batch_check_errors(self._h, C.byref(bits)), "mp_batch_check_errors")
         return bits.value
+
+    def params(self, s: int) -> PBFParams:
+        p = PBFParams()
+        check(self._lib.mp_batch_get_params(self._h, s, C.byref(p)), "mp_batch_get_params")
+        return p
+
+    def set_params(self, s: int, p: PBFParams) -> None:
+        check(self._lib.mp_batch_set_params(self._h, s, C.byref(p)), "mp_batch_set_params")
+
+    def buffer(self, which: int) -> tuple[int, int]:
+        p = C.c_void_p()
+        nb = C.c_size_t()
+        check(self._lib.mp_batch_buffer(self._h, which, C.byref(p), C.byref(nb)), "mp_batch_buffer")
+        return int(p.value or 0), int(nb.value)
+
+    def tensor(self, which: int):
+        """Zero-copy torch view of buffer `which` (all scenes' particles)."""
+        import torch
+
+        width, dtype = BUF_LAYOUT[which]
+        ptr, _ = self.buffer(which)
+        count = self.particle_count()
+        shape = (count, width) if width > 1 else (count,)
+        typestr = "<f4" if dtype == "float32" else "<i4"
+        return torch.as_tensor(_CudaArray(ptr, shape, typestr, self), device=f"cuda:{self.device}")
+
+    # ---- differentiable rollouts ----
+
+    def rollout_forward(self, steps: int, checkpoint_every: int = 10, stream=None) -> None:
+        """Advance `steps` steps keeping a checkpoint every `checkpoint_every`."""
+        check(self._lib.mp_batch_rollout_forward(self._h, int(steps), int(checkpoint_every),
+                                                 stream_handle(stream)), "mp_batch_rollout_forward")
+
+    def rollout_backward(self, dpos=None, dvel=None, stream=None):
+        """Adjoint of the last rollout_forward.  dpos, dvel: dL/d(final
+        positions, velocities) as (N, 4) float32 CUDA tensors (or None).
+        Returns (dL/dpos0, dL/dvel0, per-scene grads (S, MP_SCENE_GRADS) float64)."""
+        import torch
+
+        n, S = self.particle_count(), self.scene_count()
+        dev = torch.device("cuda", self.device)
+        out_p = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        out_v = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        out_s = torch.empty((S, _abi.MP_SCENE_GRADS), dtype=torch.float64, device=dev)
+
+        def ptr(t):
+            if t is None:
+                return None
+            assert t.is_cuda and t.dtype == torch.float32 and t.shape == (n, 4) and t.is_contiguous()
+            return C.c_void_p(t.data_ptr())
+
+        check(self._lib.mp_batch_rollout_backward(self._h, ptr(dpos), ptr(dvel), C.c_void_p(out_p.data_ptr()),
+                                                  C.c_void_p(out_v.data_ptr()), C.c_void_p(out_s.data_ptr()),
+                                                  stream_handle(stream)), "mp_batch_rollout_backward")
+        return out_p, out_v, out_s
+
+    def rollout_launch_count(self, steps: int) -> int:
+        return int(self._lib.mp_batch_rollout_launch_count(self._h, int(steps)))

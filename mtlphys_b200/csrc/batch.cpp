@@ -14,6 +14,7 @@
 
 #include "../../include/mtlphys_b200.h"
 #include "host_common.h"
+#include "pbf_adjoint.h"
 #include "pbf_batch.h"
 #include "pbf_kernels.h"
 
@@ -60,6 +61,172 @@ struct mp_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
 
+    // ---- differentiable rollouts ----
+    // One recorded step: the record arrays of the step kernel plus its own
+    // prev / sorted index / hash cell / cell start arrays.
+    struct Slot {
+        BatchRecord rec;
+        float4* x0;
+        uint32_t *sidx, *scell, *cstart;
+    };
+    // A saved state: positions, velocities and the scene table (spheres).
+    struct Saved {
+        float4 *pos, *vel;
+        SceneDev* scenes;
+    };
+    void* tape_block = nullptr;
+    std::vector<Slot> slots;
+    void* ckpt_block = nullptr;
+    std::vector<Saved> ckpts;  // checkpoints, then the saved final state
+    void* adj_block = nullptr;
+    AdjArgs adj{};
+    uint32_t roll_steps = 0, roll_every = 0;
+    bool roll_valid = false;
+
+    size_t cap_slots() const { return round_up(std::max<uint32_t>(N, 1u), 256u); }
+    static size_t al(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+    int ensure_tape(uint32_t nslots) {
+        if (slots.size() >= nslots) return MP_OK;
+        if (tape_block) cudaFree(tape_block);
+        tape_block = nullptr;
+        slots.clear();
+        const size_t cap = cap_slots(), K = iterations, v4 = cap * 16, u = cap * 4;
+        const size_t per = al(sizeof(SceneDev) * std::max<uint32_t>(S, 1u)) +
+                           al(sizeof(SphereState) * std::max<uint32_t>(S, 1u)) + al(v4) + 2 * al(u) +
+                           al((size_t(max_cells) + 1) * 4) + K * (2 * al(v4) + al(9 * u) + al(u));
+        MP_CUDA(cudaMalloc(&tape_block, per * nslots));
+        char* p = static_cast<char*>(tape_block);
+        auto take = [&](size_t bytes) {
+            char* r = p;
+            p += al(bytes);
+            return r;
+        };
+        for (uint32_t i = 0; i < nslots; ++i) {
+            Slot sl{};
+            sl.rec.scenes = reinterpret_cast<SceneDev*>(take(sizeof(SceneDev) * std::max<uint32_t>(S, 1u)));
+            sl.rec.sphere0 = reinterpret_cast<SphereState*>(take(sizeof(SphereState) * std::max<uint32_t>(S, 1u)));
+            sl.x0 = reinterpret_cast<float4*>(take(v4));
+            sl.sidx = reinterpret_cast<uint32_t*>(take(u));
+            sl.scell = reinterpret_cast<uint32_t*>(take(u));
+            sl.cstart = reinterpret_cast<uint32_t*>(take((size_t(max_cells) + 1) * 4));
+            sl.rec.lam = reinterpret_cast<float4*>(take(K * v4));
+            sl.rec.delta = reinterpret_cast<float4*>(take(K * v4));
+            sl.rec.masks = reinterpret_cast<uint32_t*>(take(K * 9 * u));
+            sl.rec.overflow = reinterpret_cast<uint32_t*>(take(K * u));
+            sl.rec.stride = uint32_t(cap);
+            if (K == 0) sl.rec.lam = sl.rec.delta = nullptr, sl.rec.masks = sl.rec.overflow = nullptr;
+            slots.push_back(sl);
+        }
+        return MP_OK;
+    }
+
+    int ensure_ckpts(uint32_t n) {
+        if (ckpts.size() >= n) return MP_OK;
+        if (ckpt_block) cudaFree(ckpt_block);
+        ckpt_block = nullptr;
+        ckpts.clear();
+        const size_t v4 = cap_slots() * 16, sc = al(sizeof(SceneDev) * std::max<uint32_t>(S, 1u));
+        const size_t per = 2 * al(v4) + sc;
+        MP_CUDA(cudaMalloc(&ckpt_block, per * n));
+        char* p = static_cast<char*>(ckpt_block);
+        for (uint32_t i = 0; i < n; ++i) {
+            Saved sv{reinterpret_cast<float4*>(p), reinterpret_cast<float4*>(p + al(v4)),
+                     reinterpret_cast<SceneDev*>(p + 2 * al(v4))};
+            ckpts.push_back(sv);
+            p += per;
+        }
+        return MP_OK;
+    }
+
+    int ensure_adjoint() {
+        if (adj_block) return MP_OK;
+        const size_t cap = cap_slots(), v4 = al(cap * 16), u = al(cap * 4);
+        const size_t gbytes = al(sizeof(double) * kGradStride * std::max<uint32_t>(S, 1u));
+        const size_t total = 8 * v4 + 5 * u + gbytes;
+        MP_CUDA(cudaMalloc(&adj_block, total));
+        MP_CUDA(cudaMemset(adj_block, 0, total));
+        char* p = static_cast<char*>(adj_block);
+        auto v = [&]() { float4* r = reinterpret_cast<float4*>(p); p += v4; return r; };
+        auto w = [&]() { char* r = p; p += u; return r; };
+        adj = AdjArgs{};
+        adj.pbar = v();
+        adj.qbar = v();
+        adj.dbar = v();
+        adj.lbar = v();
+        adj.gd = v();
+        adj.p_extra = v();
+        adj.xbar = v();
+        adj.vbar = v();
+        adj.qsc = reinterpret_cast<float*>(w());
+        adj.lam_part = reinterpret_cast<float*>(w());
+        adj.lam_extra = reinterpret_cast<float*>(w());
+        adj.ccur = reinterpret_cast<uint32_t*>(w());
+        adj.cpred = reinterpret_cast<uint32_t*>(w());
+        adj.grads = reinterpret_cast<double*>(p);
+        adj.scene_of = a.scene_of;
+        adj.n = N;
+        adj.nscenes = S;
+        adj.iterations = iterations;
+        adj.stride = uint32_t(cap);
+        adj.mask_stride = a.mask_stride;
+        return MP_OK;
+    }
+
+    void free_rollout() {
+        for (void* p : {tape_block, ckpt_block, adj_block})
+            if (p) cudaFree(p);
+        tape_block = ckpt_block = adj_block = nullptr;
+        slots.clear();
+        ckpts.clear();
+        adj = AdjArgs{};
+        roll_valid = false;
+    }
+
+    int save(const Saved& sv, cudaStream_t s) {
+        const size_t v4 = size_t(N) * 16;
+        MP_CUDA(cudaMemcpyAsync(sv.pos, a.pos, v4, cudaMemcpyDeviceToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(sv.vel, a.vel, v4, cudaMemcpyDeviceToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(sv.scenes, scenes, sizeof(SceneDev) * S, cudaMemcpyDeviceToDevice, s));
+        return MP_OK;
+    }
+    int restore(const Saved& sv, cudaStream_t s) {
+        const size_t v4 = size_t(N) * 16;
+        MP_CUDA(cudaMemcpyAsync(a.pos, sv.pos, v4, cudaMemcpyDeviceToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(a.vel, sv.vel, v4, cudaMemcpyDeviceToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(scenes, sv.scenes, sizeof(SceneDev) * S, cudaMemcpyDeviceToDevice, s));
+        return MP_OK;
+    }
+
+    // One step of every scene in one launch, kept in tape slot `i`.
+    int enqueue_recorded(uint32_t i, cudaStream_t s) {
+        const Slot& sl = slots[i];
+        BatchArgs args = a;
+        args.scene_begin = 0;
+        args.scene_end = S;
+        args.p_begin = 0;
+        args.p_end = N;
+        args.prev = sl.x0;
+        args.sidx = sl.sidx;
+        args.scell = sl.scell;
+        args.cstart = sl.cstart;
+        args.rec = sl.rec;
+        const cudaError_t e = launch_batch_step(args, block, blocks(), s);
+        if (e != cudaSuccess) return fail(MP_ERR_CUDA, "recorded step launch: %s", cudaGetErrorString(e));
+        return MP_OK;
+    }
+
+    // The reverse of the step kept in slot `i`, whose end positions are x1.
+    int enqueue_adjoint(uint32_t i, const float4* x1, cudaStream_t s) {
+        const Slot& sl = slots[i];
+        AdjArgs ad = adj;
+        ad.t = AdjStep{sl.rec.scenes, sl.rec.sphere0, sl.x0, x1, sl.sidx, sl.scell, sl.cstart,
+                       sl.rec.lam, sl.rec.delta, sl.rec.masks, sl.rec.overflow};
+        const cudaError_t e = launch_adjoint_step(ad, s);
+        if (e != cudaSuccess) return fail(MP_ERR_CUDA, "adjoint step launch: %s", cudaGetErrorString(e));
+        return MP_OK;
+    }
+
     void drop_graph() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
@@ -76,6 +243,7 @@ struct mp_batch {
     }
     ~mp_batch() {
         DeviceGuard g(device);
+        free_rollout();
         free_all();
         if (cap_stream) cudaStreamDestroy(cap_stream);
     }
@@ -115,6 +283,27 @@ struct mp_batch {
             const cudaError_t e = launch_batch_step(args, block, std::min(nb, need), s);
             if (e != cudaSuccess) return fail(MP_ERR_CUDA, "batch step launch: %s", cudaGetErrorString(e));
         }
+        return MP_OK;
+    }
+
+    // One step of every scene (graph replay in graph mode).
+    int step(cudaStream_t s) {
+        if (!graph_mode) return enqueue(s);
+        if (!gexec) {
+            if (!cap_stream) MP_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+            MP_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue(cap_stream);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(cap_stream, &g);
+            if (rc != MP_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (ce != cudaSuccess) return fail(MP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+            graph = g;
+            MP_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+        }
+        MP_CUDA(cudaGraphLaunch(gexec, s));
         return MP_OK;
     }
 
@@ -224,6 +413,7 @@ int mp_batch_reset(mp_batch* b, uint32_t nscenes, const uint32_t* counts, const 
         off += counts[s];
     }
     DeviceGuard g(b->device);
+    b->free_rollout();
     b->free_all();
     b->S = nscenes;
     b->N = uint32_t(total);
@@ -316,6 +506,7 @@ int mp_batch_set_dts(mp_batch* b, const float* dts) {
         if (!(dts[s] > 0.0f)) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u: dt must be > 0", s);
     }
     DeviceGuard g(b->device);
+    b->roll_valid = false;
     MP_CUDA(cudaDeviceSynchronize());
     // refresh the constants that depend on dt, keep the device-side sphere state
     std::vector<SceneDev> cur(b->S);
@@ -335,24 +526,8 @@ int mp_batch_set_dts(mp_batch* b, const float* dts) {
 int mp_batch_step(mp_batch* b, mp_stream stream) {
     if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
     DeviceGuard g(b->device);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (!b->graph_mode) return b->enqueue(s);
-    if (!b->gexec) {
-        if (!b->cap_stream) MP_CUDA(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
-        MP_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-        const int rc = b->enqueue(b->cap_stream);
-        cudaGraph_t graph = nullptr;
-        const cudaError_t ce = cudaStreamEndCapture(b->cap_stream, &graph);
-        if (rc != MP_OK) {
-            if (graph) cudaGraphDestroy(graph);
-            return rc;
-        }
-        if (ce != cudaSuccess) return fail(MP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-        b->graph = graph;
-        MP_CUDA(cudaGraphInstantiate(&b->gexec, b->graph, 0));
-    }
-    MP_CUDA(cudaGraphLaunch(b->gexec, s));
-    return MP_OK;
+    b->roll_valid = false;
+    return b->step(static_cast<cudaStream_t>(stream));
 }
 
 int mp_batch_set_mode(mp_batch* b, int serial) {
@@ -495,6 +670,7 @@ int mp_batch_upload(mp_batch* b, uint32_t which, const void* host, size_t count,
     if (need > bytes) return fail(MP_ERR_INVALID_ARGUMENT, "%zu elements exceed buffer %u", count, which);
     if (!need) return MP_OK;
     DeviceGuard g(b->device);
+    b->roll_valid = false;
     MP_CUDA(cudaMemcpyAsync(dptr, host, need, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream)));
     return MP_OK;
 }
@@ -525,6 +701,7 @@ int mp_batch_set_sphere(mp_batch* b, uint32_t scene, const float center[3], cons
     }
     s.r = radius;
     DeviceGuard g(b->device);
+    b->roll_valid = false;
     MP_CUDA(cudaDeviceSynchronize());
     MP_CUDA(cudaMemcpy(&b->scenes[scene].sphere, &s, sizeof(s), cudaMemcpyHostToDevice));
     return MP_OK;
@@ -543,6 +720,111 @@ int mp_batch_get_sphere(mp_batch* b, uint32_t scene, float center[3], float velo
     }
     if (radius) *radius = s.r;
     return MP_OK;
+}
+
+int mp_batch_set_params(mp_batch* b, uint32_t scene, const mp_pbf_params* params) {
+    if (!b || !params) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (scene >= b->S) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u >= %u", scene, b->S);
+    int rc = validate_params(*params);
+    if (rc != MP_OK) return rc;
+    if (params->solver_iterations != b->iterations)
+        return fail(MP_ERR_INVALID_ARGUMENT, "all scenes must use the same solver_iterations");
+    GridDev g0, g1;
+    make_grid(b->params[scene], g0);
+    rc = make_grid(*params, g1);
+    if (rc != MP_OK) return rc;
+    if (g0.dgx != g1.dgx || g0.dgy != g1.dgy || g0.dgz != g1.dgz || g0.ox != g1.ox || g0.oy != g1.oy ||
+        g0.oz != g1.oz || g0.cs != g1.cs)
+        return fail(MP_ERR_INVALID_ARGUMENT, "the hash grid (box, cell size) cannot change without a reset");
+    DeviceGuard g(b->device);
+    b->roll_valid = false;
+    MP_CUDA(cudaDeviceSynchronize());
+    SceneDev cur;
+    MP_CUDA(cudaMemcpy(&cur, &b->scenes[scene], sizeof(SceneDev), cudaMemcpyDeviceToHost));
+    cur.c = make_consts(*params, g1, b->counts[scene], b->dts[scene],
+                        b->scene_ids[scene] == MP_SCENE_SPHERE_DROP);
+    MP_CUDA(cudaMemcpy(&b->scenes[scene], &cur, sizeof(SceneDev), cudaMemcpyHostToDevice));
+    b->params[scene] = *params;
+    b->host_scenes[scene].c = cur.c;
+    b->drop_graph();
+    return MP_OK;
+}
+
+int mp_batch_get_params(const mp_batch* b, uint32_t scene, mp_pbf_params* params) {
+    if (!b || !params) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (scene >= b->S) return fail(MP_ERR_INVALID_ARGUMENT, "scene %u >= %u", scene, b->S);
+    *params = b->params[scene];
+    return MP_OK;
+}
+
+int mp_batch_rollout_forward(mp_batch* b, uint32_t steps, uint32_t checkpoint_every, mp_stream stream) {
+    if (!b || checkpoint_every == 0) return fail(MP_ERR_INVALID_ARGUMENT, "bad argument");
+    for (uint32_t s = 0; s < b->S; ++s) {
+        GridDev g0;
+        make_grid(b->params[s], g0);
+        if (g0.dgx > 2048 || g0.dgy > 2048 || g0.dgz > 1024)
+            return fail(MP_ERR_UNSUPPORTED, "scene %u: the adjoint needs a hash grid of at most "
+                        "2048 x 2048 x 1024 cells", s);
+    }
+    DeviceGuard g(b->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    b->roll_valid = false;
+    const uint32_t nck = (steps + checkpoint_every - 1) / checkpoint_every;
+    int rc = b->ensure_ckpts(nck + 1);  // + the final state, saved by the backward pass
+    for (uint32_t t = 0; rc == MP_OK && t < steps; ++t) {
+        if (t % checkpoint_every == 0) rc = b->save(b->ckpts[t / checkpoint_every], st);
+        if (rc == MP_OK) rc = b->step(st);
+    }
+    if (rc != MP_OK) return rc;
+    b->roll_steps = steps;
+    b->roll_every = checkpoint_every;
+    b->roll_valid = true;
+    return MP_OK;
+}
+
+int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel, float* dpos0, float* dvel0,
+                              double* dscene, mp_stream stream) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (!b->roll_valid)
+        return fail(MP_ERR_INVALID_ARGUMENT, "no rollout recorded since the state last changed");
+    DeviceGuard g(b->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint32_t steps = b->roll_steps, every = b->roll_every;
+    const uint32_t nck = (steps + every - 1) / every;
+    int rc = b->ensure_tape(std::min(steps, every));
+    if (rc == MP_OK) rc = b->ensure_adjoint();
+    if (rc != MP_OK) return rc;
+    const size_t v4 = size_t(b->N) * 16;
+    AdjArgs& ad = b->adj;
+    if (dpos) MP_CUDA(cudaMemcpyAsync(ad.xbar, dpos, v4, cudaMemcpyDeviceToDevice, st));
+    else MP_CUDA(cudaMemsetAsync(ad.xbar, 0, v4, st));
+    if (dvel) MP_CUDA(cudaMemcpyAsync(ad.vbar, dvel, v4, cudaMemcpyDeviceToDevice, st));
+    else MP_CUDA(cudaMemsetAsync(ad.vbar, 0, v4, st));
+    MP_CUDA(cudaMemsetAsync(ad.grads, 0, sizeof(double) * kGradStride * b->S, st));
+    const mp_batch::Saved& fin = b->ckpts[nck];
+    rc = b->save(fin, st);
+    for (uint32_t seg = nck; rc == MP_OK && seg-- > 0;) {
+        const uint32_t t0 = seg * every, t1 = std::min(steps, t0 + every);
+        rc = b->restore(b->ckpts[seg], st);
+        for (uint32_t t = t0; rc == MP_OK && t < t1; ++t) rc = b->enqueue_recorded(t - t0, st);
+        for (uint32_t t = t1; rc == MP_OK && t-- > t0;) {
+            const float4* x1 = t + 1 == t1 ? b->a.pos : b->slots[t + 1 - t0].x0;
+            rc = b->enqueue_adjoint(t - t0, x1, st);
+        }
+    }
+    if (rc == MP_OK) rc = b->restore(fin, st);
+    if (rc != MP_OK) return rc;
+    if (dpos0) MP_CUDA(cudaMemcpyAsync(dpos0, ad.xbar, v4, cudaMemcpyDeviceToDevice, st));
+    if (dvel0) MP_CUDA(cudaMemcpyAsync(dvel0, ad.vbar, v4, cudaMemcpyDeviceToDevice, st));
+    if (dscene)
+        MP_CUDA(cudaMemcpyAsync(dscene, ad.grads, sizeof(double) * kGradStride * b->S,
+                                cudaMemcpyDeviceToDevice, st));
+    return MP_OK;
+}
+
+uint32_t mp_batch_rollout_launch_count(const mp_batch* b, uint32_t steps) {
+    if (!b || b->N == 0) return 0;
+    return steps * (1u + adjoint_launch_count(b->iterations));
 }
 
 int mp_batch_check_errors(mp_batch* b, uint32_t* bits) {

@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(BS) k_batch_step(BatchArgs a) {
     for (uint32_t s = a.scene_begin + gtid; s < a.scene_end; s += gsize) {
         sc[s].bb[0] = sc[s].bb[1] = sc[s].bb[2] = 0xffffffffu;
         sc[s].bb[3] = sc[s].bb[4] = sc[s].bb[5] = 0u;
+        if (a.rec.sphere0) a.rec.sphere0[s] = sc[s].sphere;
         if (sc[s].c.sphere) sphere_advance(sc[s].c, &sc[s].sphere);
     }
     if (gtid == 0) *a.long_count = 0;
@@ -174,6 +175,8 @@ __global__ void __launch_bounds__(BS) k_batch_step(BatchArgs a) {
     grid_barrier(a.bar_count, a.bar_gen, a.err);
 
     // 3: cell id inside the scene's box + warp-aggregated count
+    if (a.rec.scenes)
+        for (uint32_t s = a.scene_begin + gtid; s < a.scene_end; s += gsize) a.rec.scenes[s] = sc[s];
     const uint32_t ncells = *a.total_cells;
     if (ncells > a.max_cells && gtid == 0) atomicOr(a.err, kDevErrIndex);
     const bool cells_ok = ncells <= a.max_cells;
@@ -276,32 +279,41 @@ __global__ void __launch_bounds__(BS) k_batch_step(BatchArgs a) {
                                  a.ncount, a.foam, a.err);
         return;
     }
+    // a recorded step keeps every lambda pass's output, row masks and
+    // corrections in the record instead of overwriting one buffer
+    const bool record = a.rec.lam != nullptr;
     for (uint32_t it = 0; it < a.iterations; ++it) {
         const bool last = it + 1 == a.iterations;
+        float4* lam_out = record ? a.rec.lam + size_t(it) * a.rec.stride : a.sorted_b;
+        const RowMasks rmi =
+            record ? RowMasks{a.rec.masks + size_t(it) * 9 * a.mask_stride,
+                              a.rec.overflow + size_t(it) * a.mask_stride, a.mask_stride}
+                   : rm;
+        float4* drec = record ? a.rec.delta + size_t(it) * a.rec.stride : nullptr;
         for (uint32_t s = pb + gtid; s < pe; s += gsize) {
             const StepConsts& c = sc[a.scene_of[s]].c;
             if (it == 0) {
                 if (last)
-                    lambda_first_item<true>(c, s, a.sorted_a, a.sorted_b, a.scell, a.cstart, a.sidx,
-                                            a.lambdas, a.ncount, rm);
+                    lambda_first_item<true>(c, s, a.sorted_a, lam_out, a.scell, a.cstart, a.sidx,
+                                            a.lambdas, a.ncount, rmi);
                 else
-                    lambda_first_item<false>(c, s, a.sorted_a, a.sorted_b, a.scell, a.cstart, a.sidx,
-                                             a.lambdas, a.ncount, rm);
+                    lambda_first_item<false>(c, s, a.sorted_a, lam_out, a.scell, a.cstart, a.sidx,
+                                             a.lambdas, a.ncount, rmi);
             } else if (last) {
-                lambda_item<true>(c, s, a.sorted_a, a.sorted_b, a.scell, a.cstart, a.sidx, a.lambdas, rm);
+                lambda_item<true>(c, s, a.sorted_a, lam_out, a.scell, a.cstart, a.sidx, a.lambdas, rmi);
             } else {
-                lambda_item<false>(c, s, a.sorted_a, a.sorted_b, a.scell, a.cstart, a.sidx, a.lambdas, rm);
+                lambda_item<false>(c, s, a.sorted_a, lam_out, a.scell, a.cstart, a.sidx, a.lambdas, rmi);
             }
         }
         grid_barrier(a.bar_count, a.bar_gen, a.err);
         for (uint32_t s = pb + gtid; s < pe; s += gsize) {
             const SceneDev& sd = sc[a.scene_of[s]];
             if (last)
-                delta_item<true>(sd.c, s, a.sorted_b, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
-                                 a.pos, a.vel, a.prev, a.ncount, a.foam, a.err, rm);
+                delta_item<true>(sd.c, s, lam_out, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
+                                 a.pos, a.vel, a.prev, a.ncount, a.foam, a.err, rmi, drec);
             else
-                delta_item<false>(sd.c, s, a.sorted_b, a.sorted_a, a.scell, a.cstart, a.sidx,
-                                  &sd.sphere, a.pos, a.vel, a.prev, a.ncount, a.foam, a.err, rm);
+                delta_item<false>(sd.c, s, lam_out, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
+                                  a.pos, a.vel, a.prev, a.ncount, a.foam, a.err, rmi, drec);
         }
         if (!last) grid_barrier(a.bar_count, a.bar_gen, a.err);
     }

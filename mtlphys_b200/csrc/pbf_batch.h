@@ -19,6 +19,19 @@ struct SceneDev {
     SphereState sphere;  // used when c.sphere != 0
 };
 
+// Recording of one step for the adjoint (lam == nullptr: not recording).
+// The step's prev, sidx, scell and cstart arrays are kept as well: for a
+// recorded step the host points BatchArgs at the record's own copies.
+struct BatchRecord {
+    SceneDev* scenes;      // scene table once the sub-grids are set (sphere advanced)
+    SphereState* sphere0;  // every scene's sphere before the advance
+    float4* lam;           // iterations x stride: (l, lambda) written by each lambda pass
+    float4* delta;         // iterations x stride: unclamped correction of each delta pass
+    uint32_t* masks;       // iterations x 9 x mask_stride: row masks of each lambda pass
+    uint32_t* overflow;    // iterations x mask_stride
+    uint32_t stride;       // slots per lam / delta array
+};
+
 struct BatchArgs {
     SceneDev* scenes;
     uint32_t scene_begin, scene_end;  // scenes of this launch
@@ -36,6 +49,7 @@ struct BatchArgs {
     uint32_t* total_cells;
     unsigned *bar_count, *bar_gen;
     uint32_t* err;
+    BatchRecord rec;
 };
 
 // Cooperative launch of one step of scenes [scene_begin, scene_end) with

@@ -281,7 +281,7 @@ __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float l
 // (3 consecutive cells, one contiguous slot range) is taken in chunks of 32
 // candidates: phase 1 loads every candidate once, does only the distance test
 // and sets a bit for each one within h; phase 2 visits just the set bits and
-// calls body(q, rx, ry, rz, r2).  The in-range body, about an eighth of the
+// calls body(k, q, rx, ry, rz, r2) with k the candidate's slot.  The in-range body, about an eighth of the
 // candidates, then runs on most lanes of the warp instead of on the few lanes
 // whose candidate happened to be in range.
 //
@@ -348,7 +348,7 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
                     const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
                     const float4 q = __ldg(&src[k]);
                     const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y), rz = __fsub_rn(oz, q.z);
-                    body(q, rx, ry, rz, dist2(rx, ry, rz));
+                    body(k, q, rx, ry, rz, dist2(rx, ry, rz));
                 }
             }
             if (masks) {
@@ -385,9 +385,8 @@ __device__ __forceinline__ void lambda_first_item(const StepConsts& c, uint32_t 
     LambdaAcc acc;
     const uint32_t cnt = sweep<false>(c, cur, cstart, cx, cy, cz, p.x, p.y, p.z, cx, cy, cz, s,
                                       rm.rows ? &rm : nullptr,
-                                      [&](const float4&, float rx, float ry, float rz, float r2) {
-                                          acc.add(c, rx, ry, rz, r2);
-                                      });
+                                      [&](uint32_t, const float4&, float rx, float ry, float rz,
+                                          float r2) { acc.add(c, rx, ry, rz, r2); });
     const float lambda = acc.lambda(c);
     // l = p - A(c): exact for the particle's own cell (Sterbenz), so the
     // anchored state starts equal to the FP32 predicted position.
@@ -417,7 +416,9 @@ __device__ __forceinline__ void lambda_item(const StepConsts& c, uint32_t s,
             __fadd_rn(anchor_z(c.g, pcz), l.z), cx, cy, cz);
     LambdaAcc acc;
     sweep<true>(c, cur, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s, rm.rows ? &rm : nullptr,
-                [&](const float4&, float rx, float ry, float rz, float r2) { acc.add(c, rx, ry, rz, r2); });
+                [&](uint32_t, const float4&, float rx, float ry, float rz, float r2) {
+                    acc.add(c, rx, ry, rz, r2);
+                });
     const float lambda = acc.lambda(c);
     nxt[s] = make_float4(l.x, l.y, l.z, lambda);
     if (LAST) lambdas[sidx[s]] = lambda;
@@ -475,8 +476,49 @@ __device__ __forceinline__ void finalize_particle(const StepConsts& c, uint32_t 
     if (!(isfinite(X + Y + Z) && isfinite(vx + vy + vz))) atomicOr(err, kDevErrNaN);
 }
 
+// The in-range pairs a lambda pass recorded in its row masks (rows of at most
+// 32 candidates; the particle's own bit cleared), walked with the anchored
+// neighbour vector of sweep<true>: body(k, q, rx, ry, rz, r2) for each.
+// (cx, cy, cz): the stencil cell of the particle at offset l from anchor
+// (ax, ay, az).
+template <class Body>
+__device__ __forceinline__ void masked_pairs(const StepConsts& c, const float4* __restrict__ src,
+                                             const uint32_t* __restrict__ cstart, const RowMasks& rm,
+                                             uint32_t s, const float4& l, float ax, float ay, float az,
+                                             int cx, int cy, int cz, Body&& body) {
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, c.g.gx - 1);
+    const int y0 = max(cy - 1, 0), y1 = min(cy + 1, c.g.gy - 1);
+    const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
+    const int nx = x1 - x0 + 1;
+    if (nx <= 0) return;
+    const float ox0 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0)), l.x);
+    const float ox1 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 1)), l.x);
+    const float ox2 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 2)), l.x);
+    for (int z = z0; z <= z1; ++z) {
+        const float oz = __fadd_rn(__fsub_rn(az, anchor_z(c.g, z)), l.z);
+        for (int y = y0; y <= y1; ++y) {
+            uint32_t mask = rm.rows[uint32_t((z - z0) * 3 + (y - y0)) * rm.stride + s];
+            if (mask == 0u) continue;
+            const float oy = __fadd_rn(__fsub_rn(ay, anchor_y(c.g, y)), l.y);
+            const uint32_t base = cell_hash(c.g, x0, y, z);
+            const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
+            const uint32_t b2 = nx > 1 ? cstart[base + 2] : b1;
+            while (mask) {
+                const uint32_t k = b0 + uint32_t(__ffs(mask) - 1);
+                mask &= mask - 1;
+                const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
+                const float4 q = __ldg(&src[k]);
+                const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y);
+                const float rz = __fsub_rn(oz, q.z);
+                body(k, q, rx, ry, rz, dist2(rx, ry, rz));
+            }
+        }
+    }
+}
+
 // applyDeltaSorted + sphereCollision on the anchored state; the last
-// iteration also scatters back, finalizes and writes foam.
+// iteration also scatters back, finalizes and writes foam.  drec (may be
+// NULL): receives the particle's unclamped correction, for the adjoint.
 template <bool LAST>
 __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
                                            const float4* __restrict__ src, float4* __restrict__ dst,
@@ -488,7 +530,7 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
                                            const float4* __restrict__ prev,
                                            const uint32_t* __restrict__ ncount,
                                            float* __restrict__ foam, uint32_t* err,
-                                           const RowMasks& rm) {
+                                           const RowMasks& rm, float4* __restrict__ drec) {
     const float4 l = src[s];
     int pcx, pcy, pcz;
     decode_cell(c.g, scell[s], pcx, pcy, pcz);
@@ -496,47 +538,18 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
     int cx, cy, cz;
     cell_of(c.g, __fadd_rn(ax, l.x), __fadd_rn(ay, l.y), __fadd_rn(az, l.z), cx, cy, cz);
     float dx = 0.0f, dy = 0.0f, dz = 0.0f;
-    auto body = [&](const float4& q, float rx, float ry, float rz, float r2) {
+    auto body = [&](uint32_t, const float4& q, float rx, float ry, float rz, float r2) {
         delta_add(c, l.w, q.w, rx, ry, rz, r2, dx, dy, dz);
     };
-    if (rm.rows != nullptr && rm.overflow[s] == 0u) {
-        // the lambda pass's in-range bits, row by row (rows fit one chunk)
-        const int x0 = max(cx - 1, 0), x1 = min(cx + 1, c.g.gx - 1);
-        const int y0 = max(cy - 1, 0), y1 = min(cy + 1, c.g.gy - 1);
-        const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
-        const int nx = x1 - x0 + 1;
-        if (nx > 0) {
-            const float ox0 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0)), l.x);
-            const float ox1 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 1)), l.x);
-            const float ox2 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 2)), l.x);
-            for (int z = z0; z <= z1; ++z) {
-                const float oz = __fadd_rn(__fsub_rn(az, anchor_z(c.g, z)), l.z);
-                for (int y = y0; y <= y1; ++y) {
-                    uint32_t mask = rm.rows[uint32_t((z - z0) * 3 + (y - y0)) * rm.stride + s];
-                    if (mask == 0u) continue;
-                    const float oy = __fadd_rn(__fsub_rn(ay, anchor_y(c.g, y)), l.y);
-                    const uint32_t base = cell_hash(c.g, x0, y, z);
-                    const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
-                    const uint32_t b2 = nx > 1 ? cstart[base + 2] : b1;
-                    while (mask) {
-                        const uint32_t k = b0 + uint32_t(__ffs(mask) - 1);
-                        mask &= mask - 1;
-                        const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
-                        const float4 q = __ldg(&src[k]);
-                        const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y);
-                        const float rz = __fsub_rn(oz, q.z);
-                        body(q, rx, ry, rz, dist2(rx, ry, rz));
-                    }
-                }
-            }
-        }
-    } else {
+    if (rm.rows != nullptr && rm.overflow[s] == 0u)
+        masked_pairs(c, src, cstart, rm, s, l, ax, ay, az, cx, cy, cz, body);
+    else
         sweep<true>(c, src, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s,
                     static_cast<const RowMasks*>(nullptr), body);
-    }
     dx = __fmul_rn(dx, c.inv_rho0);
     dy = __fmul_rn(dy, c.inv_rho0);
     dz = __fmul_rn(dz, c.inv_rho0);
+    if (drec) drec[s] = make_float4(dx, dy, dz, 0.0f);
     const float dl = __fsqrt_rn(dist2(dx, dy, dz));
     if (dl > c.max_step) {
         const float f = __fdiv_rn(c.max_step, dl);

@@ -53,7 +53,7 @@ k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < c.n)
         delta_item<LAST>(c, s, src, dst, scell, cstart, sidx, sphere, pos, vel, prev, ncount, foam,
-                         err, rm);
+                         err, rm, nullptr);
 }
 
 __global__ void __launch_bounds__(256)

@@ -1,0 +1,293 @@
+"""Adjoint of the PBF step on the GPU (mp_batch_rollout_*, the
+torch.autograd.Function in mtlphys_b200.autograd).
+
+  * one step: the CUDA adjoint equals the FP64 numpy adjoint restatement
+    (oracle/adjoint_ref.py, itself pinned to the C++ oracle and to finite
+    differences by test_adjoint_ref.py) on the same FP32 input state;
+  * rollouts: gradients through 60 checkpointed steps equal central finite
+    differences of FP64 oracle rollouts within 1e-3 relative (directional
+    derivative for the per-particle initial velocities, dL/dk for s_corr k,
+    dL/d v0 for the sphere's initial speed);
+  * the checkpoint interval does not change the gradients; the state after
+    the backward pass is the state the forward pass ended in.
+
+Conditioning.  The benchmark parameters (s_corr k = 0.1, CFM epsilon = 100)
+make these scenes explode within a few steps; finite differences of the FP64
+oracle itself then do not converge beyond one step, so the rollout checks
+run the same geometry at k = 1e-4, epsilon = 1e4, where they converge to
+four or more digits.  Single steps are also checked at k = 0.1.
+"""
+import numpy as np
+import pytest
+
+from mtlphys_b200 import _abi, configs
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 120.0
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def make_batch(params, descs, counts, scenes=None, dts=None):
+    from mtlphys_b200.batch import Batch
+
+    b = Batch(0)
+    b.reset(counts, params, dts or [DT] * len(counts), scenes, descs)
+    return b
+
+
+# ---- one step against the numpy restatement ---------------------------------------
+
+from test_adjoint_ref import CASES, scene  # noqa: E402
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_one_step_adjoint_matches_the_fp64_restatement(cuda, name):
+    from oracle import adjoint_ref as A
+
+    torch = _torch()
+    kw, sphere = CASES[name]
+    p, x, v = scene(**kw)
+    n = len(x)
+    d = configs.lattice((kw["side"],) * 3, kw["origin"], 1)
+    sid = _abi.MP_SCENE_SPHERE_DROP if sphere is not None else _abi.MP_SCENE_CUBE_DROP
+    b = make_batch([p], [d], [n], [sid])
+    dev = torch.device("cuda", 0)
+    pos0 = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    vel0 = torch.zeros_like(pos0)
+    pos0[:, :3] = torch.tensor(x, dtype=torch.float32)
+    vel0[:, :3] = torch.tensor(v, dtype=torch.float32)
+    b.tensor(_abi.MP_BUF_POSITIONS).copy_(pos0)
+    b.tensor(_abi.MP_BUF_VELOCITIES).copy_(vel0)
+    if sphere is not None:
+        b.set_sphere(0, sphere[:3], sphere[3:6], sphere[6])
+    b.rollout_forward(1, 1)
+    rng = np.random.default_rng(9)
+    wx, wv = rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    gp = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    gv = torch.zeros_like(gp)
+    gp[:, :3] = torch.tensor(wx, dtype=torch.float32)
+    gv[:, :3] = torch.tensor(wv, dtype=torch.float32)
+    dp, dv, ds = b.rollout_backward(gp, gv)
+    torch.cuda.synchronize()
+    assert b.check_errors() == 0
+    # the same step in FP64 from the same FP32 state
+    c = A.consts(p, DT)
+    s7 = None
+    if sphere is not None:
+        s7 = np.array(sphere, np.float64)
+        A.sphere_advance(p, DT, s7)
+    xin = pos0[:, :3].double().cpu().numpy()
+    vin = vel0[:, :3].double().cpu().numpy()
+    _, _, tape = A.forward(c, xin, vin, s7)
+    xb, vb, kb, cb, rb = A.adjoint(c, tape, wx, wv)
+    rel = lambda a, r: np.linalg.norm(a - r) / np.linalg.norm(r)
+    assert rel(dp[:, :3].double().cpu().numpy(), xb) < 1e-3
+    assert rel(dv[:, :3].double().cpu().numpy(), vb) < 1e-3
+    g = ds.cpu().numpy()[0]
+    assert abs(g[_abi.MP_GRAD_SCORR_K] - kb) <= 1e-3 * abs(kb)
+    if sphere is not None:
+        # through this step's push and the kinematic advance before it
+        sb = np.zeros(7)
+        sb[:3] = cb
+        sb[6] = rb
+        s0 = np.array(sphere, np.float64)
+        rec = A.sphere_advance(p, DT, s0.copy())
+        want = A.sphere_advance_adjoint(p, DT, rec, sb)
+        np.testing.assert_allclose(g[1:8], want, rtol=1e-3, atol=1e-3 * np.abs(want).max())
+    b.close()
+
+
+# ---- rollouts against finite differences of the FP64 oracle ------------------------
+
+def cube_params():
+    p = configs.base_params(3)
+    p.scorr_k = 1e-4
+    p.epsilon = 1e4
+    return p
+
+
+def oracle_rollout(p, pos0, vel0, steps, sphere=None):
+    from oracle import oracle as O
+
+    x = np.ascontiguousarray(pos0[:, :3], dtype=np.float64)
+    v = np.ascontiguousarray(vel0[:, :3], dtype=np.float64)
+    s = None if sphere is None else np.array(sphere, np.float64)
+    for _ in range(steps):
+        O.step_f64(p, DT, x, v, s)
+    return x
+
+
+@pytest.fixture(scope="module")
+def cube_case():
+    """The 20^3 differentiable cube drop (60 steps), its FP64 target run
+    (initial velocities N(0, 0.5 m/s)) and FD references."""
+    from oracle import oracle as O
+
+    w = configs.diff_cube(side=20, steps=60)
+    p = cube_params()
+    pos0 = O.seed_scene(p, w.scene, w.n, w.desc)
+    rng = np.random.default_rng(5)
+    vt = rng.normal(0.0, 0.5, size=(w.n, 3))
+    target = oracle_rollout(p, pos0, vt, w.steps)
+    u = rng.normal(size=(w.n, 3))
+    zero = np.zeros((w.n, 3))
+
+    def loss(v0, k=None):
+        q = cube_params()
+        if k is not None:
+            q.scorr_k = k
+        return float(np.mean(np.sum((oracle_rollout(q, pos0, v0, w.steps) - target) ** 2, axis=1)))
+
+    e = 1e-6
+    fd_u = (loss(e * u) - loss(-e * u)) / (2 * e)
+    ek = 1e-5 * p.scorr_k
+    fd_k = (loss(zero, p.scorr_k + ek) - loss(zero, p.scorr_k - ek)) / (2 * ek)
+    return {"w": w, "p": p, "pos0": pos0, "target": target, "u": u, "fd_u": fd_u, "fd_k": fd_k,
+            "loss0": loss(zero)}
+
+
+def gpu_cube_gradients(case, every):
+    torch = _torch()
+    from mtlphys_b200.autograd import rollout
+
+    w, p = case["w"], case["p"]
+    b = make_batch([p], [w.desc], [w.n])
+    dev = torch.device("cuda", 0)
+    pos0 = torch.tensor(case["pos0"], dtype=torch.float32, device=dev)
+    vel0 = torch.zeros((w.n, 4), dtype=torch.float32, device=dev, requires_grad=True)
+    k = torch.tensor([p.scorr_k], dtype=torch.float64, requires_grad=True)
+    pos, _ = rollout(b, w.steps, pos0, vel0, scorr_k=k, checkpoint_every=every)
+    target = torch.tensor(case["target"], dtype=torch.float64, device=dev)
+    loss = ((pos[:, :3].double() - target) ** 2).sum(1).mean()
+    loss.backward()
+    torch.cuda.synchronize()
+    assert b.check_errors() == 0
+    final = pos.detach().clone()
+    after = b.tensor(_abi.MP_BUF_POSITIONS).clone()
+    b.close()
+    return {"loss": float(loss), "gv": vel0.grad[:, :3].double().cpu().numpy(), "gk": float(k.grad[0]),
+            "final": final, "after": after}
+
+
+def test_rollout_gradients_match_fp64_finite_differences(cuda, cube_case):
+    g = gpu_cube_gradients(cube_case, every=10)
+    assert abs(g["loss"] - cube_case["loss0"]) <= 1e-3 * cube_case["loss0"]
+    an_u = float(np.sum(g["gv"] * cube_case["u"]))
+    assert abs(an_u - cube_case["fd_u"]) <= 1e-3 * abs(cube_case["fd_u"]), (an_u, cube_case["fd_u"])
+    assert abs(g["gk"] - cube_case["fd_k"]) <= 1e-3 * abs(cube_case["fd_k"]), (g["gk"], cube_case["fd_k"])
+    # the backward pass leaves the state where the forward pass ended
+    torch = _torch()
+    assert torch.equal(g["final"], g["after"])
+
+
+def test_checkpoint_interval_does_not_change_gradients(cuda, cube_case):
+    ref = gpu_cube_gradients(cube_case, every=10)
+    for every in (1, 7, 60):
+        g = gpu_cube_gradients(cube_case, every=every)
+        assert g["loss"] == ref["loss"]
+        np.testing.assert_allclose(g["gv"], ref["gv"], rtol=0, atol=1e-6 * np.abs(ref["gv"]).max())
+        assert abs(g["gk"] - ref["gk"]) <= 1e-6 * abs(ref["gk"])
+
+
+def test_sphere_drop_gradients_match_fp64_finite_differences(cuda):
+    """A sphere pushed into a small lake: dL/d(initial vertical speed) and
+    dL/d(radius) of the mean squared height of the 200 highest particles of
+    a target run, 15 steps, against FD of FP64 oracle rollouts.  FD of the
+    radius is itself only good to ~0.2% here (particles crossing the sphere
+    surface switch cells), hence its looser bound."""
+    torch = _torch()
+    from oracle import oracle as O
+    from mtlphys_b200.autograd import rollout
+
+    H = configs.H
+    side, layers, steps, r0 = 9, 20, 15, 0.12
+    width = (side - 1) * 0.5 * H + H
+    p = cube_params()
+    p.set(bounds_min=(0.0, 0.0, 0.0), bounds_max=(width, 40 * H, width))
+    p.sphere_radius = r0
+    d = configs.lattice((side, layers, side), (0.5 * H, 0.5 * H, 0.5 * H), 77)
+    n = side * side * layers
+    pos0 = O.seed_scene(p, _abi.MP_SCENE_SPHERE_DROP, n, d)
+    top = float(pos0[:, 1].max())
+    sphere = lambda vy, r: [width / 2, top + r + 0.02, width / 2, 0.0, vy, 0.0, r]
+    target = oracle_rollout(p, pos0, np.zeros((n, 3)), steps, sphere(-1.5, r0))
+    surf = np.argsort(-target[:, 1])[:200]
+
+    def loss(vy, r):
+        x = oracle_rollout(p, pos0, np.zeros((n, 3)), steps, sphere(vy, r))
+        return float(np.mean((x[surf, 1] - target[surf, 1]) ** 2))
+
+    e = 1e-5
+    fd_v = (loss(-1.0 + e, r0) - loss(-1.0 - e, r0)) / (2 * e)
+    fd_r = (loss(-1.0, r0 + e) - loss(-1.0, r0 - e)) / (2 * e)
+
+    b = make_batch([p], [d], [n], [_abi.MP_SCENE_SPHERE_DROP])
+    dev = torch.device("cuda", 0)
+    s0 = sphere(-1.0, r0)
+    c = torch.tensor([s0[:3]], dtype=torch.float64, requires_grad=True)
+    v = torch.tensor([s0[3:6]], dtype=torch.float64, requires_grad=True)
+    r = torch.tensor([r0], dtype=torch.float64, requires_grad=True)
+    pos, _ = rollout(b, steps, torch.tensor(pos0, device=dev), torch.zeros((n, 4), device=dev),
+                     sphere=(c, v, r), checkpoint_every=5)
+    idx = torch.tensor(surf, device=dev)
+    tgt = torch.tensor(target[surf, 1], dtype=torch.float64, device=dev)
+    L = ((pos[idx, 1].double() - tgt) ** 2).mean()
+    L.backward()
+    assert b.check_errors() == 0
+    assert abs(float(v.grad[0, 1]) - fd_v) <= 1e-3 * abs(fd_v), (float(v.grad[0, 1]), fd_v)
+    assert abs(float(r.grad[0]) - fd_r) <= 1e-2 * abs(fd_r), (float(r.grad[0]), fd_r)
+    b.close()
+
+
+def test_batched_scenes_get_their_single_scene_gradients(cuda):
+    """Three uneven scenes in one batch: each scene's gradients equal those
+    of the same scene alone (the scenes do not interact)."""
+    torch = _torch()
+    from mtlphys_b200.autograd import rollout
+
+    w = configs.batch_cubes(num=3, lo=300, hi=3000, steps=8)
+    for p in w.params:
+        p.scorr_k = 1e-4
+        p.epsilon = 1e4
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(2)
+
+    def run(idx):
+        b = make_batch([w.params[i] for i in idx], [w.descs[i] for i in idx], [w.counts[i] for i in idx],
+                       dts=[w.dts[i] for i in idx])
+        n = b.particle_count()
+        pos0 = b.tensor(_abi.MP_BUF_POSITIONS).clone()
+        vel0 = torch.zeros((n, 4), device=dev, requires_grad=True)
+        k = torch.tensor([w.params[i].scorr_k for i in idx], dtype=torch.float64, requires_grad=True)
+        pos, vel = rollout(b, w.steps, pos0, vel0, scorr_k=k, checkpoint_every=3)
+        wts = torch.tensor(rng_weights[np.concatenate([np.arange(offs[i], offs[i] + w.counts[i]) for i in idx])],
+                           dtype=torch.float64, device=dev)
+        (pos[:, :3].double() * wts).sum().backward()
+        out = (vel0.grad[:, :3].cpu().numpy(), k.grad.numpy())
+        b.close()
+        return out
+
+    offs = np.concatenate([[0], np.cumsum(w.counts)])
+    rng_weights = rng.normal(size=(int(offs[-1]), 3))
+    gv_all, gk_all = run([0, 1, 2])
+    for s in range(3):
+        gv, gk = run([s])
+        np.testing.assert_allclose(gv_all[offs[s]:offs[s + 1]], gv, rtol=0, atol=1e-6 * np.abs(gv).max())
+        assert abs(gk_all[s] - gk[0]) <= 1e-9 * abs(gk[0])
+
+
+def test_backward_after_a_state_change_is_refused(cuda):
+    w = configs.diff_cube(side=6, steps=3)
+    b = make_batch([cube_params()], [w.desc], [w.n])
+    b.rollout_forward(3, 2)
+    b.rollout_backward()
+    b.step()
+    with pytest.raises(_abi.MPError):
+        b.rollout_backward()
+    b.close()
