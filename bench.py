@@ -299,6 +299,7 @@ def run_ours(args, world, rank, local) -> dict | None:
     e.close()
 
     batched = None if args.no_batch else run_batched(args, world, rank, local, stream, flush_l2)
+    adjoint = None if args.no_adjoint else run_adjoint(args, world, rank, local, stream)
 
     if rank != 0:
         return None
@@ -322,9 +323,117 @@ def run_ours(args, world, rank, local) -> dict | None:
     if batched is not None:
         line["batched"] = batched
         line["gpu_launches"] += batched["launches_timed"]
+    if adjoint is not None:
+        line["adjoint"] = adjoint
+        line["gpu_launches"] += adjoint.pop("launches_timed")
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args)
     return line
+
+
+def run_adjoint(args, world, rank, local, stream) -> dict:
+    """Cost of the gradient relative to the forward rollout it differentiates:
+    backward ms (the recomputation of every 10-step segment with the steps
+    recorded, and the adjoint kernels) / forward ms (the rollout with its
+    checkpoints), both CUDA-event timed on the engine's stream, max over
+    ranks.  Workloads: the 97,336-particle differentiable cube drop (60
+    steps; loss = mean squared distance to the final positions of a seeded
+    run with initial velocities N(0, 0.5 m/s); gradients w.r.t. every initial
+    velocity and s_corr k) at the benchmark parameters and at the
+    well-conditioned ones the gradient checks use; and the 32-scene batched
+    sphere drop (40 steps, all scenes in one launch per step; gradients
+    w.r.t. every scene's sphere state and radius)."""
+    import torch
+
+    from mtlphys_b200 import _abi, configs
+    from mtlphys_b200.batch import Batch
+    from mtlphys_b200.ensemble import shard_workload
+
+    reps = max(1, min(3, args.steps))
+    out = {}
+    launches = 0
+
+    def time_rollout(b, steps, every, pos0, vel0, target, reset=None):
+        nonlocal launches
+        n = b.particle_count()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        fwd = bwd = 0.0
+        for r in range(reps + 1):  # the first repetition warms up
+            if reset is not None:
+                reset()
+            with torch.cuda.stream(stream):
+                b.tensor(_abi.MP_BUF_POSITIONS).copy_(pos0)
+                b.tensor(_abi.MP_BUF_VELOCITIES).copy_(vel0)
+            dist_barrier(world)
+            torch.cuda.synchronize()
+            ev[0].record(stream)
+            b.rollout_forward(steps, every, stream)
+            ev[1].record(stream)
+            with torch.cuda.stream(stream):  # dL/dx(T) of the mean squared distance
+                g = (b.tensor(_abi.MP_BUF_POSITIONS) - target) * (2.0 / max(n, 1))
+                g[:, 3] = 0.0
+            ev[2].record(stream)
+            b.rollout_backward(g, None, stream)
+            ev[3].record(stream)
+            torch.cuda.synchronize()
+            if r > 0:
+                fwd += ev[0].elapsed_time(ev[1])
+                bwd += ev[2].elapsed_time(ev[3])
+                launches += steps + b.rollout_launch_count(steps)
+        if b.check_errors():
+            raise RuntimeError("device error in the adjoint leg")
+        fwd = dist_max(fwd / reps, world)
+        bwd = dist_max(bwd / reps, world)
+        return {"forward_ms": round(fwd, 3), "backward_ms": round(bwd, 3), "ratio": round(bwd / fwd, 3)}
+
+    def target_of(b, steps, pos0, vel_t):
+        with torch.cuda.stream(stream):
+            b.tensor(_abi.MP_BUF_POSITIONS).copy_(pos0)
+            b.tensor(_abi.MP_BUF_VELOCITIES).copy_(vel_t)
+        for _ in range(steps):
+            b.step(stream)
+        torch.cuda.synchronize()
+        return b.tensor(_abi.MP_BUF_POSITIONS).clone()
+
+    dev = torch.device("cuda", local)
+    gen = torch.Generator(device=dev)
+    for label, k, cfm in (("benchmark_params", None, None), ("conditioned", 1e-4, 1e5)):
+        w = configs.diff_cube(side=46, steps=60)
+        if k is not None:
+            w.params.scorr_k = k
+            w.params.epsilon = cfm
+        b = Batch(local)
+        b.reset([w.n], [w.params], [w.dt], [w.scene], [w.desc])
+        b.set_graph_mode(True)
+        pos0 = b.tensor(_abi.MP_BUF_POSITIONS).clone()
+        gen.manual_seed(configs.SEED_BASE + 2)
+        vel_t = torch.zeros((w.n, 4), device=dev)
+        vel_t[:, :3] = torch.randn((w.n, 3), device=dev, generator=gen) * 0.5
+        target = target_of(b, w.steps, pos0, vel_t)
+        t = time_rollout(b, w.steps, 10, pos0, torch.zeros_like(vel_t), target)
+        out[label] = {"workload": "diff_cube", "particles": w.n, "steps": w.steps, "checkpoint_every": 10,
+                      "scorr_k": float(w.params.scorr_k), "epsilon": float(w.params.epsilon), **t}
+        b.close()
+    full = configs.batch_spheres()
+    ws, _ = shard_workload(full, rank, world)
+    b = Batch(local)
+    b.reset(ws.counts, ws.params, ws.dts, ws.scenes, ws.descs)
+    b.set_graph_mode(True)
+    pos0 = b.tensor(_abi.MP_BUF_POSITIONS).clone()
+    zero = torch.zeros_like(pos0)
+    target = target_of(b, ws.steps, pos0, zero)  # spheres from their seeded starts
+    def spheres_start():  # the optimised run: each sphere's initial speed halved
+        for s, sph in enumerate(ws.spheres):
+            b.set_sphere(s, sph[:3], (sph[3], 0.5 * sph[4], sph[5]), sph[6])
+
+    t = time_rollout(b, ws.steps, 10, pos0, zero, target, spheres_start)
+    out["batched_sphere_drop"] = {"workload": "batch_spheres", "scenes": len(full.counts),
+                                  "particles": full.n, "steps": ws.steps, "checkpoint_every": 10, **t}
+    b.close()
+    out["what"] = ("backward (recompute of each checkpointed segment with the steps recorded + adjoint "
+                   "kernels) / forward rollout with checkpoints")
+    out["launches_timed"] = launches
+    return out
 
 
 def run_batched(args, world, rank, local, stream, flush_l2) -> dict:
@@ -375,14 +484,58 @@ def run_batched(args, world, rank, local, stream, flush_l2) -> dict:
                      "scenes_per_s": round(len(full.counts) * 1000.0 / ms, 1),
                      "launch": {"block": tune["block"], "blocks_per_sm": tune["blocks_per_sm"]},
                      "launches_per_step": launches}
+    ranges = [b.scene_range(s) for s in range(len(w.counts))]
     b.close()
+
+    # the single-scene engine (the multi-kernel step: 5 + 2K launches in a
+    # CUDA graph), one engine per scene, stepped one scene after another
+    from mtlphys_b200 import Engine
+
+    engines = []
+    for s in range(len(w.counts)):
+        e = Engine(local)
+        e.set_params(w.params[s])
+        e.reset(w.counts[s], w.scenes[s], w.descs[s])
+        e.set_graph_mode(True)
+        engines.append(e)
+    for _ in range(args.warmup):
+        for s, e in enumerate(engines):
+            e.step(w.dts[s], stream)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    for i in range(steps):
+        flush_l2()
+        starts[i].record(stream)
+        for s, e in enumerate(engines):
+            e.step(w.dts[s], stream)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    ms = dist_max(sum(s.elapsed_time(t) for s, t in zip(starts, ends)) / steps, world)
+    same_engine = True
+    for s, e in enumerate(engines):
+        f, n = ranges[s]
+        same_engine &= bool(np.array_equal(e.positions(), finals["batched"][0][f:f + n]))
+        e.close()
+    k_it = int(w.params[0].solver_iterations) if w.params else 0
+    per_scene = 5 + 2 * k_it
+    res["engines"] = {"ms_per_step": round(ms, 4), "scenes_per_s": round(len(full.counts) * 1000.0 / ms, 1),
+                      "launches_per_step": per_scene * sum(1 for c in w.counts if c > 0),
+                      "what": "one single-scene engine per scene (multi-kernel step in a CUDA graph), "
+                              "stepped one after another"}
+
     same = all(np.array_equal(x, y) for x, y in zip(finals["batched"], finals["serial"]))
     return {"workload": full.describe(), "steps": steps, "warmup": args.warmup,
-            "batched": res["batched"], "serial": res["serial"],
+            "batched": res["batched"], "serial": res["serial"], "engines": res["engines"],
             "speedup": round(res["serial"]["ms_per_step"] / res["batched"]["ms_per_step"], 3),
+            "speedup_vs_engines": round(res["engines"]["ms_per_step"] / res["batched"]["ms_per_step"], 3),
             "bit_identical": bool(dist_max(0.0 if same else 1.0, world) == 0.0),
+            "bit_identical_engines": bool(dist_max(0.0 if same_engine else 1.0, world) == 0.0),
             "l2": "flushed between timed steps", "mode": "CUDA graph replay",
-            "launches_timed": steps * (res["batched"]["launches_per_step"] + res["serial"]["launches_per_step"])}
+            "launches_timed": steps * (res["batched"]["launches_per_step"] + res["serial"]["launches_per_step"]
+                                       + res["engines"]["launches_per_step"])}
 
 
 def read_traffic(kernel: str):
@@ -486,6 +639,7 @@ def main() -> None:
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
