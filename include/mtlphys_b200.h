@@ -102,6 +102,9 @@ typedef struct mp_pbf_params {
     float    sphere_gravity;     /* -9.81                 (Engine.cpp:694)         */
     float    sphere_drag;        /* 0.998 per step        (Engine.cpp:695-697)     */
     float    sphere_restitution; /* 0.4                   (Engine.cpp:702-707)     */
+    float    integrate_damping;  /* 0.999 legacy integrator (Engine.cpp:584)      */
+    float    integrate_restitution; /* 0.4                (Integrate.metal:29)      */
+    float    mouse_falloff;      /* 0.4: exp(-r^2/(R^2 f)) (Constraints.metal:250)  */
 } mp_pbf_params;
 
 /*
@@ -200,6 +203,20 @@ int mp_engine_buffer(mp_engine* e, uint32_t which, void** dptr, size_t* bytes);
  * and returns once the host memory may be reused; download synchronizes. */
 int mp_engine_upload(mp_engine* e, uint32_t which, const void* host, size_t count, mp_stream stream);
 int mp_engine_download(mp_engine* e, uint32_t which, void* host, size_t count, mp_stream stream);
+/* Engine::integrate(cmd, dt) (Engine.cpp:578-596, Integrate.metal:11-42): the
+ * legacy semi-implicit Euler step with box bounds, kept by the reference for
+ * its integrator tests: v = (v + g dt) * integrate_damping, p += v dt, then
+ * per axis a position outside [bounds_min, bounds_max] is clamped and its
+ * velocity reflected with integrate_restitution.  Asynchronous on `stream`;
+ * dt <= 0 is a no-op. */
+int mp_engine_integrate(mp_engine* e, float dt, mp_stream stream);
+/* Engine::applyMousePulse(cmd, rayOrigin, rayDir, force, radius)
+ * (Engine.cpp:813-841, Constraints.metal:231-253): every particle in front of
+ * the ray origin within `radius` of the ray (ray_dir normalized by the
+ * caller) gets force * exp(-r^2 / (radius^2 mouse_falloff)) added to its
+ * velocity.  Asynchronous on `stream`. */
+int mp_engine_apply_mouse_pulse(mp_engine* e, const float ray_origin[3], const float ray_dir[3],
+                                const float force[3], float radius, mp_stream stream);
 /* Sphere state of scene 2 (Engine.hpp:182-184). */
 int mp_engine_set_sphere(mp_engine* e, const float center[3], const float velocity[3], float radius);
 int mp_engine_get_sphere(mp_engine* e, float center[3], float velocity[3], float* radius);

@@ -87,6 +87,9 @@ class PBFParams(C.Structure):
         ("sphere_gravity", C.c_float),
         ("sphere_drag", C.c_float),
         ("sphere_restitution", C.c_float),
+        ("integrate_damping", C.c_float),
+        ("integrate_restitution", C.c_float),
+        ("mouse_falloff", C.c_float),
     ]
 
     def copy(self) -> "PBFParams":
@@ -169,6 +172,9 @@ PROTOTYPES = {
     "mp_engine_get_sphere": (_INT, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                     C.POINTER(C.c_float)]),
     "mp_engine_check_errors": (_INT, [_VP, C.POINTER(_U32)]),
+    "mp_engine_integrate": (_INT, [_VP, C.c_float, _VP]),
+    "mp_engine_apply_mouse_pulse": (_INT, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                           C.POINTER(C.c_float), C.c_float, _VP]),
     "mp_engine_synchronize": (_INT, [_VP]),
     "mp_batch_create": (_INT, [_INT, C.POINTER(_VP)]),
     "mp_batch_destroy": (_INT, [_VP]),

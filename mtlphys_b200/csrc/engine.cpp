@@ -227,6 +227,9 @@ void fill_default_params(mp_pbf_params& p) {
     p.sphere_gravity = -9.81f;     // Engine.cpp:694
     p.sphere_drag = 0.998f;        // Engine.cpp:695-697
     p.sphere_restitution = 0.4f;   // Engine.cpp:702-707
+    p.integrate_damping = 0.999f;  // Engine.cpp:584
+    p.integrate_restitution = 0.4f;  // Integrate.metal:29
+    p.mouse_falloff = 0.4f;        // Constraints.metal:250
 }
 
 void fill_default_desc(mp_scene_desc& d) {
@@ -814,6 +817,52 @@ int mp_engine_get_sphere(mp_engine* e, float center[3], float velocity[3], float
         if (velocity) velocity[a] = s.v[a];
     }
     if (radius) *radius = s.r;
+    return MP_OK;
+}
+
+int mp_engine_integrate(mp_engine* e, float dt, mp_stream stream) {
+    if (!e) return fail(MP_ERR_INVALID_ARGUMENT, "NULL engine");
+    if (!(dt > 0.0f)) return MP_OK;
+    DeviceGuard g(e->device);
+    const mp_pbf_params& p = e->params;
+    mpb::IntegrateConsts c{};
+    c.n = e->n;
+    c.dt = dt;
+    c.damping = p.integrate_damping;
+    c.restitution = p.integrate_restitution;
+    c.gx = p.gravity[0];
+    c.gy = p.gravity[1];
+    c.gz = p.gravity[2];
+    c.bminx = p.bounds_min[0];
+    c.bminy = p.bounds_min[1];
+    c.bminz = p.bounds_min[2];
+    c.bmaxx = p.bounds_max[0];
+    c.bmaxy = p.bounds_max[1];
+    c.bmaxz = p.bounds_max[2];
+    const cudaError_t err = mpb::launch_integrate(c, e->d.pos, e->d.vel, static_cast<cudaStream_t>(stream));
+    if (err != cudaSuccess) return fail(MP_ERR_CUDA, "integrate launch: %s", cudaGetErrorString(err));
+    return MP_OK;
+}
+
+int mp_engine_apply_mouse_pulse(mp_engine* e, const float ray_origin[3], const float ray_dir[3],
+                                const float force[3], float radius, mp_stream stream) {
+    if (!e || !ray_origin || !ray_dir || !force) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    DeviceGuard g(e->device);
+    mpb::MouseConsts c{};
+    c.n = e->n;
+    c.ox = ray_origin[0];
+    c.oy = ray_origin[1];
+    c.oz = ray_origin[2];
+    c.dx = ray_dir[0];
+    c.dy = ray_dir[1];
+    c.dz = ray_dir[2];
+    c.fx = force[0];
+    c.fy = force[1];
+    c.fz = force[2];
+    c.radius = radius;
+    c.falloff = e->params.mouse_falloff;
+    const cudaError_t err = mpb::launch_mouse_pulse(c, e->d.vel, e->d.pos, static_cast<cudaStream_t>(stream));
+    if (err != cudaSuccess) return fail(MP_ERR_CUDA, "mouse pulse launch: %s", cudaGetErrorString(err));
     return MP_OK;
 }
 

@@ -83,6 +83,23 @@ cudaError_t launch_solver(const StepConsts& c, const DevState& d, uint32_t itera
 // Number of kernel launches one step issues (for the benchmark's count).
 uint32_t step_launch_count(uint32_t iterations);
 
+// Legacy integrator (Integrate.metal SimParams, Shared.h:28-35).
+struct IntegrateConsts {
+    uint32_t n;
+    float dt, damping, restitution;
+    float gx, gy, gz;
+    float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
+};
+cudaError_t launch_integrate(const IntegrateConsts& c, float4* pos, float4* vel, cudaStream_t s);
+
+// Mouse pulse (MousePulseUniforms, Constraints.metal:222-229).
+struct MouseConsts {
+    uint32_t n;
+    float ox, oy, oz, dx, dy, dz, fx, fy, fz;
+    float radius, falloff;
+};
+cudaError_t launch_mouse_pulse(const MouseConsts& c, float4* vel, const float4* pos, cudaStream_t s);
+
 // Sets the message mp_last_error() returns on this thread.
 void record_error(const char* msg);
 

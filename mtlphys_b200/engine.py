@@ -253,6 +253,19 @@ class Engine:
         check(self._lib.mp_engine_get_sphere(self._h, c, v, C.byref(r)), "mp_engine_get_sphere")
         return np.array([c[0], c[1], c[2], v[0], v[1], v[2], r.value], np.float32)
 
+    def integrate(self, dt: float, stream=None) -> None:
+        """Engine::integrate: the legacy semi-implicit Euler step with box bounds."""
+        check(self._lib.mp_engine_integrate(self._h, C.c_float(dt), stream_handle(stream)),
+              "mp_engine_integrate")
+
+    def apply_mouse_pulse(self, ray_origin, ray_dir, force, radius: float, stream=None) -> None:
+        """Engine::applyMousePulse: add force * exp(-r^2 / (R^2 falloff)) to the
+        velocities of particles within `radius` of the ray (ray_dir normalized)."""
+        v3 = lambda a: (C.c_float * 3)(*[float(x) for x in a])
+        check(self._lib.mp_engine_apply_mouse_pulse(self._h, v3(ray_origin), v3(ray_dir), v3(force),
+                                                    C.c_float(radius), stream_handle(stream)),
+              "mp_engine_apply_mouse_pulse")
+
     def set_sphere(self, center, velocity, radius: float) -> None:
         c = (C.c_float * 3)(*center)
         v = (C.c_float * 3)(*velocity)

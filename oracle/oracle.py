@@ -77,6 +77,11 @@ def lib() -> C.CDLL:
                                     C.c_uint32, _F]
         L.or_sphere_advance.argtypes = [C.POINTER(PBFParams), C.c_double, _D]
         L.or_sphere_advance.restype = None
+        L.or_integrate_f32.argtypes = [C.POINTER(PBFParams), C.c_float, C.c_uint32, _F, _F]
+        L.or_integrate_f32.restype = None
+        L.or_mouse_pulse_f32.argtypes = [C.POINTER(PBFParams), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                         C.POINTER(C.c_float), C.c_float, C.c_uint32, _F, _F]
+        L.or_mouse_pulse_f32.restype = None
         L.or_step.argtypes = [C.POINTER(PBFParams), C.c_float, C.c_uint32, _F, _F, C.c_void_p,
                               C.POINTER(StepOut)]
         L.or_step_f64.argtypes = [C.POINTER(PBFParams), C.c_double, C.c_uint32, _D, _D, C.c_void_p]
@@ -210,6 +215,22 @@ def step(p: PBFParams, dt: float, pos4, vel4, sphere=None) -> dict:
     if sphere is not None:
         sphere[:] = sph
     return o
+
+
+def integrate_f32(p: PBFParams, dt: float, pos4, vel4):
+    """Engine::integrate in FP32; returns new (pos4, vel4) arrays."""
+    pos4, vel4 = _f4(pos4).copy(), _f4(vel4).copy()
+    lib().or_integrate_f32(C.byref(p), C.c_float(dt), len(pos4), pos4, vel4)
+    return pos4, vel4
+
+
+def mouse_pulse_f32(p: PBFParams, origin, direction, force, radius: float, pos4, vel4):
+    """Engine::applyMousePulse in FP32; returns the new velocities."""
+    vel4 = _f4(vel4).copy()
+    v3 = lambda a: (C.c_float * 3)(*[float(x) for x in a])
+    lib().or_mouse_pulse_f32(C.byref(p), v3(origin), v3(direction), v3(force), C.c_float(radius),
+                             len(vel4), _f4(pos4), vel4)
+    return vel4
 
 
 def step_f64(p: PBFParams, dt: float, pos3, vel3, sphere=None) -> None:

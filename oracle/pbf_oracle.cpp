@@ -525,6 +525,62 @@ int or_seed_scene(const mp_pbf_params* p, uint32_t scene, const mp_scene_desc* d
     return 0;
 }
 
+// Legacy integrator: kernel integrate (engine/shaders/Integrate.metal:11-42)
+// as Engine::integrate dispatches it (Engine.cpp:578-596), in FP32 with one
+// rounding per operation in the shader's order.
+void or_integrate_f32(const mp_pbf_params* p, float dt, uint32_t n, float* pos4, float* vel4) {
+    const float rest = p->integrate_restitution, damp = p->integrate_damping;
+    for (uint32_t i = 0; i < n; ++i) {
+        float* q = pos4 + 4 * size_t(i);
+        float* v = vel4 + 4 * size_t(i);
+        for (int a = 0; a < 3; ++a) {
+            volatile float gdt = p->gravity[a] * dt;
+            volatile float va = v[a] + gdt;
+            v[a] = va * damp;
+            volatile float step = v[a] * dt;
+            q[a] = q[a] + step;
+        }
+        for (int a = 0; a < 3; ++a)
+            if (q[a] < p->bounds_min[a]) { q[a] = p->bounds_min[a]; v[a] = -v[a] * rest; }
+        for (int a = 0; a < 3; ++a)
+            if (q[a] > p->bounds_max[a]) { q[a] = p->bounds_max[a]; v[a] = -v[a] * rest; }
+        q[3] = 1.0f;
+        v[3] = 0.0f;
+    }
+}
+
+// kernel applyMousePulse (Constraints.metal:231-253) in FP32, dot products
+// summed x + y, then + z.
+void or_mouse_pulse_f32(const mp_pbf_params* p, const float origin[3], const float dir[3],
+                        const float force[3], float radius, uint32_t n, const float* pos4,
+                        float* vel4) {
+    auto dot = [](const float* a, const float* b) {
+        volatile float xy = a[0] * b[0] + a[1] * b[1];
+        return xy + a[2] * b[2];
+    };
+    const float R2 = radius * radius;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* q = pos4 + 4 * size_t(i);
+        float toP[3];
+        for (int a = 0; a < 3; ++a) toP[a] = q[a] - origin[a];
+        const float t = dot(toP, dir);
+        if (t <= 0.0f) continue;
+        float d[3];
+        for (int a = 0; a < 3; ++a) {
+            volatile float c = origin[a] + dir[a] * t;
+            d[a] = q[a] - c;
+        }
+        const float r2 = dot(d, d);
+        if (r2 < R2) {
+            volatile float den = R2 * p->mouse_falloff;
+            const float intensity = std::exp(-r2 / den);
+            float* v = vel4 + 4 * size_t(i);
+            for (int a = 0; a < 3; ++a) v[a] = v[a] + force[a] * intensity;
+            v[3] = 0.0f;
+        }
+    }
+}
+
 void or_sphere_advance(const mp_pbf_params* p, double dt, double* s) {
     or_grid g;
     if (or_make_grid(p, &g) != 0) return;

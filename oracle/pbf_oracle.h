@@ -65,6 +65,15 @@ void or_predict_f32(const float* pos4, const float* vel4, uint32_t n, const floa
 int or_seed_scene(const mp_pbf_params* p, uint32_t scene, const mp_scene_desc* d,
                   uint32_t n, float* pos4);
 
+/* Engine::integrate (Engine.cpp:578-596, Integrate.metal:11-42) in FP32, in
+ * place on n float4 positions / velocities. */
+void or_integrate_f32(const mp_pbf_params* p, float dt, uint32_t n, float* pos4, float* vel4);
+/* Engine::applyMousePulse (Engine.cpp:813-841, Constraints.metal:231-253) in
+ * FP32, in place on n float4 velocities. */
+void or_mouse_pulse_f32(const mp_pbf_params* p, const float origin[3], const float dir[3],
+                        const float force[3], float radius, uint32_t n, const float* pos4,
+                        float* vel4);
+
 /* Sphere kinematics of Engine::step (Engine.cpp:693-712) in FP64.
  * s = {cx, cy, cz, vx, vy, vz, radius}. */
 void or_sphere_advance(const mp_pbf_params* p, double dt, double* s);

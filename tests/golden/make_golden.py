@@ -121,6 +121,38 @@ def main() -> None:
     fx["integrate/bounce/pos"] = pos.copy()
     fx["integrate/bounce/vel"] = vel.copy()
 
+    # ---- legacy integrator and mouse pulse on many particles (the reference's
+    # shaders, one dispatch each), inputs inside, on and outside the box ----
+    rng = np.random.default_rng(0x6D7470687973 + 17)
+    n = 1024
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform([-3.5, -3.5, -3.5], [3.5, 6.5, 3.5], size=(n, 3))
+    pos[:, 3] = 1.0
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0.0, 4.0, size=(n, 3))
+    fx["integrate/many/pos_in"] = pos.copy()
+    fx["integrate/many/vel_in"] = vel.copy()
+    for _ in range(3):
+        O.ref().ref_integrate(pos, vel, ga, C.c_float(1.0 / 60.0), lo, hi, C.c_float(0.999), n)
+    fx["integrate/many/pos"] = pos.copy()
+    fx["integrate/many/vel"] = vel.copy()
+    origin = (C.c_float * 3)(0.5, 2.0, -6.0)
+    d = np.array([0.1, -0.05, 1.0], np.float64)
+    d /= np.linalg.norm(d)
+    direction = (C.c_float * 3)(*[float(x) for x in d])
+    force = (C.c_float * 3)(1.5, 3.0, -0.5)
+    ppos = np.zeros((n, 4), np.float32)
+    ppos[:, :3] = rng.uniform([-3, -3, -9], [3, 6, 3], size=(n, 3))
+    ppos[:, 3] = 1.0
+    pvel = np.zeros((n, 4), np.float32)
+    pvel[:, :3] = rng.normal(0.0, 1.0, size=(n, 3))
+    fx["mouse/pos"] = ppos.copy()
+    fx["mouse/vel_in"] = pvel.copy()
+    fx["mouse/ray"] = np.array([list(origin), list(direction), list(force)], np.float32)
+    fx["mouse/radius"] = np.float32(1.2)
+    O.ref().ref_k_mouse_pulse(pvel, ppos, origin, direction, force, C.c_float(1.2), n, n)
+    fx["mouse/vel"] = pvel.copy()
+
     path = os.path.join(OUT, "reference_shaders.npz")
     np.savez_compressed(path, **fx)
     print(f"wrote {path}: {len(fx)} arrays, {os.path.getsize(path)} bytes")
