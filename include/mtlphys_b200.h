@@ -308,6 +308,24 @@ int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel,
  * included). */
 uint32_t mp_batch_rollout_launch_count(const mp_batch* b, uint32_t steps);
 
+/* ---- state snapshots (no reference counterpart: the reference keeps its
+ *      state only in its Metal buffers) ------------------------------------------
+ * A snapshot is a self-describing byte string: a 64-byte header ("MTLPSNAP",
+ * version, kind, scene and particle counts, struct sizes), one record per
+ * scene (mp_pbf_params, mp_scene_desc, scene id, particle count, dt, sphere
+ * center/velocity/radius), then every particle's position and velocity
+ * (float4, original order).  *_snapshot_size gives the bytes needed;
+ * *_snapshot waits for queued work and copies the state into `host`;
+ * *_restore re-creates the engine or batch from a snapshot (parameters,
+ * scenes, buffers, state), after which stepping continues exactly as from
+ * the saved state.  mtlphys_b200/snapshot.py reads and writes the format. */
+size_t mp_engine_snapshot_size(const mp_engine* e);
+int mp_engine_snapshot(mp_engine* e, void* host, size_t bytes);
+int mp_engine_restore(mp_engine* e, const void* host, size_t bytes);
+size_t mp_batch_snapshot_size(const mp_batch* b);
+int mp_batch_snapshot(mp_batch* b, void* host, size_t bytes);
+int mp_batch_restore(mp_batch* b, const void* host, size_t bytes);
+
 /* ---- scan: Engine.hpp:92-100 --------------------------------------------- */
 /* runExclusiveScan(cmd, in, out, chunkSums, n) (Engine.cpp:843-882): out[i]
  * = sum of in[0..i) modulo 2^32, single pass with decoupled look-back; no

@@ -202,6 +202,12 @@ PROTOTYPES = {
     "mp_batch_rollout_forward": (_INT, [_VP, _U32, _U32, _VP]),
     "mp_batch_rollout_backward": (_INT, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "mp_batch_rollout_launch_count": (_U32, [_VP, _U32]),
+    "mp_engine_snapshot_size": (_SZ, [_VP]),
+    "mp_engine_snapshot": (_INT, [_VP, _VP, _SZ]),
+    "mp_engine_restore": (_INT, [_VP, _VP, _SZ]),
+    "mp_batch_snapshot_size": (_SZ, [_VP]),
+    "mp_batch_snapshot": (_INT, [_VP, _VP, _SZ]),
+    "mp_batch_restore": (_INT, [_VP, _VP, _SZ]),
     "mp_exclusive_scan_scratch_bytes": (_SZ, [_U32]),
     "mp_exclusive_scan": (_INT, [_VP, _VP, _U32, _VP, _SZ, _VP]),
     "mp_exclusive_scan_noalloc": (_INT, [_VP, _VP, _U32, _VP]),

@@ -130,6 +130,27 @@ class Batch:
         check(self._lib.mp_batch_check_errors(self._h, C.byref(bits)), "mp_batch_check_errors")
         return bits.value
 
+    # ---- state snapshots ----
+    def snapshot_bytes(self) -> bytes:
+        """The engine state as a snapshot byte string (waits for queued work)."""
+        size = int(self._lib.mp_batch_snapshot_size(self._h))
+        buf = (C.c_char * size)()
+        check(self._lib.mp_batch_snapshot(self._h, buf, size), "mp_batch_snapshot")
+        return bytes(buf)
+
+    def restore_bytes(self, data: bytes) -> None:
+        """Re-create the state saved in a snapshot byte string."""
+        buf = C.create_string_buffer(bytes(data), len(data))
+        check(self._lib.mp_batch_restore(self._h, buf, len(data)), "mp_batch_restore")
+
+    def save(self, path: str) -> None:
+        with open(path, "wb") as f:
+            f.write(self.snapshot_bytes())
+
+    def load(self, path: str) -> None:
+        with open(path, "rb") as f:
+            self.restore_bytes(f.read())
+
     def params(self, s: int) -> PBFParams:
         p = PBFParams()
         check(self._lib.mp_batch_get_params(self._h, s, C.byref(p)), "mp_batch_get_params")

@@ -17,6 +17,7 @@
 #include "pbf_adjoint.h"
 #include "pbf_batch.h"
 #include "pbf_kernels.h"
+#include "snapshot.h"
 
 using namespace mpb;
 
@@ -45,6 +46,7 @@ struct mp_batch {
     uint32_t S = 0, N = 0, n_alloc = 0, iterations = 0;
     std::vector<uint32_t> counts, p0, scene_ids;
     std::vector<mp_pbf_params> params;
+    std::vector<mp_scene_desc> descs;
     std::vector<float> dts;
     std::vector<SceneDev> host_scenes;
     uint32_t max_cells = 0;
@@ -422,6 +424,11 @@ int mp_batch_reset(mp_batch* b, uint32_t nscenes, const uint32_t* counts, const 
     b->scene_ids.assign(nscenes, MP_SCENE_CUBE_DROP);
     if (scene_ids) b->scene_ids.assign(scene_ids, scene_ids + nscenes);
     b->params.assign(params, params + nscenes);
+    b->descs.resize(nscenes);
+    for (uint32_t s = 0; s < nscenes; ++s) {
+        if (descs) b->descs[s] = descs[s];
+        else fill_default_desc(b->descs[s]);
+    }
     b->dts.assign(dts, dts + nscenes);
     b->p0.resize(nscenes);
     for (uint32_t s = 0; s < nscenes; ++s) b->p0[s] = hs[s].p0;
@@ -825,6 +832,83 @@ int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel,
 uint32_t mp_batch_rollout_launch_count(const mp_batch* b, uint32_t steps) {
     if (!b || b->N == 0) return 0;
     return steps * (1u + adjoint_launch_count(b->iterations));
+}
+
+size_t mp_batch_snapshot_size(const mp_batch* b) {
+    return b ? mpb::snapshot_bytes(b->S, b->N) : 0;
+}
+
+int mp_batch_snapshot(mp_batch* b, void* host, size_t bytes) {
+    if (!b || !host) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    const size_t need = mpb::snapshot_bytes(b->S, b->N);
+    if (bytes < need) return fail(MP_ERR_INVALID_ARGUMENT, "snapshot needs %zu bytes, got %zu", need, bytes);
+    DeviceGuard g(b->device);
+    MP_CUDA(cudaDeviceSynchronize());
+    char* out = static_cast<char*>(host);
+    mpb::SnapshotHeader h;
+    mpb::snapshot_header(h, mpb::kSnapshotBatch, b->S, b->N);
+    std::memcpy(out, &h, sizeof(h));
+    std::vector<SceneDev> cur(b->S);
+    if (b->S) MP_CUDA(cudaMemcpy(cur.data(), b->scenes, sizeof(SceneDev) * b->S, cudaMemcpyDeviceToHost));
+    for (uint32_t s = 0; s < b->S; ++s) {
+        mpb::SnapshotScene sc;
+        std::memset(&sc, 0, sizeof(sc));
+        sc.params = b->params[s];
+        sc.desc = b->descs[s];
+        sc.scene_id = b->scene_ids[s];
+        sc.count = b->counts[s];
+        sc.dt = b->dts[s];
+        for (int a = 0; a < 3; ++a) {
+            sc.sphere[a] = cur[s].sphere.c[a];
+            sc.sphere[3 + a] = cur[s].sphere.v[a];
+        }
+        sc.sphere[6] = cur[s].sphere.r;
+        std::memcpy(out + sizeof(h) + s * sizeof(sc), &sc, sizeof(sc));
+    }
+    char* arrays = out + sizeof(h) + size_t(b->S) * sizeof(mpb::SnapshotScene);
+    if (b->N) {
+        MP_CUDA(cudaMemcpy(arrays, b->a.pos, 16 * size_t(b->N), cudaMemcpyDeviceToHost));
+        MP_CUDA(cudaMemcpy(arrays + 16 * size_t(b->N), b->a.vel, 16 * size_t(b->N), cudaMemcpyDeviceToHost));
+    }
+    return MP_OK;
+}
+
+int mp_batch_restore(mp_batch* b, const void* host, size_t bytes) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (const char* why = mpb::snapshot_check(host, bytes, mpb::kSnapshotBatch))
+        return fail(MP_ERR_INVALID_ARGUMENT, "%s", why);
+    const char* in = static_cast<const char*>(host);
+    mpb::SnapshotHeader h;
+    std::memcpy(&h, in, sizeof(h));
+    std::vector<mpb::SnapshotScene> sc(h.nscenes);
+    uint64_t total = 0;
+    for (uint32_t s = 0; s < h.nscenes; ++s) {
+        std::memcpy(&sc[s], in + sizeof(h) + s * sizeof(mpb::SnapshotScene), sizeof(mpb::SnapshotScene));
+        total += sc[s].count;
+    }
+    if (total != h.particles) return fail(MP_ERR_INVALID_ARGUMENT, "snapshot particle counts disagree");
+    std::vector<uint32_t> counts(h.nscenes), ids(h.nscenes);
+    std::vector<mp_pbf_params> params(h.nscenes);
+    std::vector<mp_scene_desc> descs(h.nscenes);
+    std::vector<float> dts(h.nscenes);
+    for (uint32_t s = 0; s < h.nscenes; ++s) {
+        counts[s] = sc[s].count;
+        ids[s] = sc[s].scene_id;
+        params[s] = sc[s].params;
+        descs[s] = sc[s].desc;
+        dts[s] = sc[s].dt;
+    }
+    int rc = mp_batch_reset(b, h.nscenes, counts.data(), ids.data(), params.data(), descs.data(), dts.data());
+    if (rc != MP_OK) return rc;
+    DeviceGuard g(b->device);
+    const char* arrays = in + sizeof(h) + size_t(h.nscenes) * sizeof(mpb::SnapshotScene);
+    if (b->N) {
+        MP_CUDA(cudaMemcpy(b->a.pos, arrays, 16 * size_t(b->N), cudaMemcpyHostToDevice));
+        MP_CUDA(cudaMemcpy(b->a.vel, arrays + 16 * size_t(b->N), 16 * size_t(b->N), cudaMemcpyHostToDevice));
+    }
+    for (uint32_t s = 0; s < h.nscenes && rc == MP_OK; ++s)
+        rc = mp_batch_set_sphere(b, s, sc[s].sphere, sc[s].sphere + 3, sc[s].sphere[6]);
+    return rc;
 }
 
 int mp_batch_check_errors(mp_batch* b, uint32_t* bits) {

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "host_common.h"
+#include "snapshot.h"
 #include "pbf_kernels.h"
 
 using namespace mpb;
@@ -864,6 +865,65 @@ int mp_engine_apply_mouse_pulse(mp_engine* e, const float ray_origin[3], const f
     const cudaError_t err = mpb::launch_mouse_pulse(c, e->d.vel, e->d.pos, static_cast<cudaStream_t>(stream));
     if (err != cudaSuccess) return fail(MP_ERR_CUDA, "mouse pulse launch: %s", cudaGetErrorString(err));
     return MP_OK;
+}
+
+size_t mp_engine_snapshot_size(const mp_engine* e) {
+    return e ? mpb::snapshot_bytes(1, e->n) : 0;
+}
+
+int mp_engine_snapshot(mp_engine* e, void* host, size_t bytes) {
+    if (!e || !host) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    const size_t need = mpb::snapshot_bytes(1, e->n);
+    if (bytes < need) return fail(MP_ERR_INVALID_ARGUMENT, "snapshot needs %zu bytes, got %zu", need, bytes);
+    DeviceGuard g(e->device);
+    MP_CUDA(cudaDeviceSynchronize());
+    char* out = static_cast<char*>(host);
+    mpb::SnapshotHeader h;
+    mpb::snapshot_header(h, mpb::kSnapshotEngine, 1, e->n);
+    std::memcpy(out, &h, sizeof(h));
+    mpb::SnapshotScene sc;
+    std::memset(&sc, 0, sizeof(sc));
+    sc.params = e->params;
+    sc.desc = e->desc;
+    sc.scene_id = e->scene;
+    sc.count = e->n;
+    mpb::SphereState sph{};
+    MP_CUDA(cudaMemcpy(&sph, e->d.sphere, sizeof(sph), cudaMemcpyDeviceToHost));
+    for (int a = 0; a < 3; ++a) {
+        sc.sphere[a] = sph.c[a];
+        sc.sphere[3 + a] = sph.v[a];
+    }
+    sc.sphere[6] = sph.r;
+    std::memcpy(out + sizeof(h), &sc, sizeof(sc));
+    char* arrays = out + sizeof(h) + sizeof(sc);
+    if (e->n) {
+        MP_CUDA(cudaMemcpy(arrays, e->d.pos, 16 * size_t(e->n), cudaMemcpyDeviceToHost));
+        MP_CUDA(cudaMemcpy(arrays + 16 * size_t(e->n), e->d.vel, 16 * size_t(e->n), cudaMemcpyDeviceToHost));
+    }
+    return MP_OK;
+}
+
+int mp_engine_restore(mp_engine* e, const void* host, size_t bytes) {
+    if (!e) return fail(MP_ERR_INVALID_ARGUMENT, "NULL engine");
+    if (const char* why = mpb::snapshot_check(host, bytes, mpb::kSnapshotEngine))
+        return fail(MP_ERR_INVALID_ARGUMENT, "%s", why);
+    const char* in = static_cast<const char*>(host);
+    mpb::SnapshotHeader h;
+    std::memcpy(&h, in, sizeof(h));
+    if (h.nscenes != 1) return fail(MP_ERR_INVALID_ARGUMENT, "an engine snapshot holds one scene");
+    mpb::SnapshotScene sc;
+    std::memcpy(&sc, in + sizeof(h), sizeof(sc));
+    if (sc.count != h.particles) return fail(MP_ERR_INVALID_ARGUMENT, "snapshot particle counts disagree");
+    int rc = mp_engine_set_params(e, &sc.params);
+    if (rc == MP_OK) rc = mp_engine_reset_scene(e, sc.count, sc.scene_id, &sc.desc);
+    if (rc != MP_OK) return rc;
+    DeviceGuard g(e->device);
+    const char* arrays = in + sizeof(h) + sizeof(sc);
+    if (e->n) {
+        MP_CUDA(cudaMemcpy(e->d.pos, arrays, 16 * size_t(e->n), cudaMemcpyHostToDevice));
+        MP_CUDA(cudaMemcpy(e->d.vel, arrays + 16 * size_t(e->n), 16 * size_t(e->n), cudaMemcpyHostToDevice));
+    }
+    return mp_engine_set_sphere(e, sc.sphere, sc.sphere + 3, sc.sphere[6]);
 }
 
 int mp_engine_check_errors(mp_engine* e, uint32_t* bits) {

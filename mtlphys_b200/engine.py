@@ -266,6 +266,27 @@ class Engine:
                                                     C.c_float(radius), stream_handle(stream)),
               "mp_engine_apply_mouse_pulse")
 
+    # ---- state snapshots ----
+    def snapshot_bytes(self) -> bytes:
+        """The engine state as a snapshot byte string (waits for queued work)."""
+        size = int(self._lib.mp_engine_snapshot_size(self._h))
+        buf = (C.c_char * size)()
+        check(self._lib.mp_engine_snapshot(self._h, buf, size), "mp_engine_snapshot")
+        return bytes(buf)
+
+    def restore_bytes(self, data: bytes) -> None:
+        """Re-create the state saved in a snapshot byte string."""
+        buf = C.create_string_buffer(bytes(data), len(data))
+        check(self._lib.mp_engine_restore(self._h, buf, len(data)), "mp_engine_restore")
+
+    def save(self, path: str) -> None:
+        with open(path, "wb") as f:
+            f.write(self.snapshot_bytes())
+
+    def load(self, path: str) -> None:
+        with open(path, "rb") as f:
+            self.restore_bytes(f.read())
+
     def set_sphere(self, center, velocity, radius: float) -> None:
         c = (C.c_float * 3)(*center)
         v = (C.c_float * 3)(*velocity)
