@@ -217,6 +217,46 @@ int mp_engine_integrate(mp_engine* e, float dt, mp_stream stream);
  * velocity.  Asynchronous on `stream`. */
 int mp_engine_apply_mouse_pulse(mp_engine* e, const float ray_origin[3], const float ray_dir[3],
                                 const float force[3], float radius, mp_stream stream);
+/* ---- headless rendering: Engine::render (Engine.cpp:884-1020) ------------
+ * The reference draws its particles with a Metal screen-space-fluid pipeline
+ * (engine/shaders/Render.metal) into the app's drawable.  Here the same
+ * passes run as CUDA kernels into device image buffers, no graphics API:
+ * sphere-billboard depth (closest wins) and additive thickness, a masked
+ * 9x9 Gaussian of the depth, the composite (normals from screen derivatives,
+ * reflected / refracted procedural sky, Beer-Lambert absorption, Schlick
+ * Fresnel, sun glint), then the box wireframe, the sphere (scene 2) and foam
+ * sprites.  The output is linear RGBA float in [0, 1] per pixel, row-major
+ * with y = 0 on the top row (the reference's target stores the same values
+ * as 8-bit sRGB). */
+typedef struct mp_render_params {
+    uint32_t size;               /* sizeof(mp_render_params)                     */
+    uint32_t width, height;      /* pixels                                       */
+    uint32_t flags;              /* MP_RENDER_* passes after the composite       */
+    float    eye[3], target[3];  /* lookAt(eye, target, +y)  (Engine.cpp:894-899) */
+    float    fov_y;              /* 1.0 rad                  (Engine.cpp:893)    */
+    float    z_near, z_far;      /* 0.1, 100                 (Engine.cpp:900)    */
+    float    particle_radius;    /* 0.022 * 1.3              (Engine.cpp:26, 902) */
+    float    foam_radius_scale;  /* 0.25                     (Render.metal:363)  */
+} mp_render_params;
+#define MP_RENDER_BOX     1u  /* bounding-box wireframe (Engine.cpp:985-995)  */
+#define MP_RENDER_SPHERE  2u  /* the sphere, scene 2 only (:997-1008)          */
+#define MP_RENDER_FOAM    4u  /* foam sprites (:1010-1018)                     */
+/* Image buffers of the last render (mp_engine_render_buffer). */
+#define MP_RENDER_BUF_COLOR     0u  /* float4[W*H] linear RGBA                    */
+#define MP_RENDER_BUF_DEPTH     1u  /* float[W*H]  closest view distance, 3.39e38 = none */
+#define MP_RENDER_BUF_SMOOTHED  2u  /* float[W*H]  smoothed view distance, 0 = none */
+#define MP_RENDER_BUF_THICKNESS 3u  /* float[W*H]  summed thickness              */
+#define MP_RENDER_BUF_NDC_DEPTH 4u  /* float[W*H]  NDC depth of the final image  */
+/* Defaults: 1280 x 720, the app's start-up orbit camera
+ * (app/MetalView.swift:93-96), all passes. */
+int mp_default_render_params(mp_render_params* rp);
+/* The camera matrices of a render (column-major 4x4): no GPU needed. */
+int mp_render_camera(const mp_render_params* rp, float view[16], float proj[16]);
+/* Render the engine's current particles.  rgba: device buffer of
+ * width * height float4 to receive the image, or NULL (then read it with
+ * mp_engine_render_buffer).  Asynchronous on `stream`. */
+int mp_engine_render(mp_engine* e, const mp_render_params* rp, float* rgba, mp_stream stream);
+int mp_engine_render_buffer(mp_engine* e, uint32_t which, void** dptr, size_t* bytes);
 /* Sphere state of scene 2 (Engine.hpp:182-184). */
 int mp_engine_set_sphere(mp_engine* e, const float center[3], const float velocity[3], float radius);
 int mp_engine_get_sphere(mp_engine* e, float center[3], float velocity[3], float* radius);

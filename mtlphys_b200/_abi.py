@@ -31,6 +31,15 @@ MP_GRAD_CENTER = 1
 MP_GRAD_VELOCITY = 4
 MP_GRAD_RADIUS = 7
 
+MP_RENDER_BOX = 1
+MP_RENDER_SPHERE = 2
+MP_RENDER_FOAM = 4
+MP_RENDER_BUF_COLOR = 0
+MP_RENDER_BUF_DEPTH = 1
+MP_RENDER_BUF_SMOOTHED = 2
+MP_RENDER_BUF_THICKNESS = 3
+MP_RENDER_BUF_NDC_DEPTH = 4
+
 MP_BUF_POSITIONS = 0
 MP_BUF_VELOCITIES = 1
 MP_BUF_PREV_POSITIONS = 2
@@ -130,6 +139,15 @@ class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint32), ("ms", C.c_double)]
 
 
+class RenderParams(C.Structure):
+    """mp_render_params."""
+
+    _fields_ = [("size", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("flags", C.c_uint32),
+                ("eye", C.c_float * 3), ("target", C.c_float * 3), ("fov_y", C.c_float),
+                ("z_near", C.c_float), ("z_far", C.c_float), ("particle_radius", C.c_float),
+                ("foam_radius_scale", C.c_float)]
+
+
 class BatchTuning(C.Structure):
     """mp_batch_tuning."""
 
@@ -202,6 +220,10 @@ PROTOTYPES = {
     "mp_batch_rollout_forward": (_INT, [_VP, _U32, _U32, _VP]),
     "mp_batch_rollout_backward": (_INT, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "mp_batch_rollout_launch_count": (_U32, [_VP, _U32]),
+    "mp_default_render_params": (_INT, [C.POINTER(RenderParams)]),
+    "mp_render_camera": (_INT, [C.POINTER(RenderParams), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "mp_engine_render": (_INT, [_VP, C.POINTER(RenderParams), _VP, _VP]),
+    "mp_engine_render_buffer": (_INT, [_VP, _U32, C.POINTER(_VP), C.POINTER(_SZ)]),
     "mp_engine_snapshot_size": (_SZ, [_VP]),
     "mp_engine_snapshot": (_INT, [_VP, _VP, _SZ]),
     "mp_engine_restore": (_INT, [_VP, _VP, _SZ]),
@@ -252,6 +274,28 @@ def default_params() -> PBFParams:
     p = PBFParams()
     check(load().mp_default_params(C.byref(p)), "mp_default_params")
     return p
+
+
+def default_render_params(**kw) -> RenderParams:
+    rp = RenderParams()
+    check(load().mp_default_render_params(C.byref(rp)), "mp_default_render_params")
+    for k, v in kw.items():
+        cur = getattr(rp, k)
+        if isinstance(cur, C.Array):
+            for i, x in enumerate(v):
+                cur[i] = x
+        else:
+            setattr(rp, k, v)
+    return rp
+
+
+def render_camera(rp: RenderParams):
+    """(view, proj) of a render as row-major 4x4 float32 numpy matrices."""
+    import numpy as np
+
+    v, p = (C.c_float * 16)(), (C.c_float * 16)()
+    check(load().mp_render_camera(C.byref(rp), v, p), "mp_render_camera")
+    return (np.array(v[:], np.float32).reshape(4, 4).T.copy(), np.array(p[:], np.float32).reshape(4, 4).T.copy())
 
 
 def default_scene_desc() -> SceneDesc:

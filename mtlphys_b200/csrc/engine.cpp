@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "host_common.h"
+#include "pbf_render.h"
 #include "snapshot.h"
 #include "pbf_kernels.h"
 
@@ -380,6 +381,27 @@ struct mp_engine {
     float graph_dt = 0.0f;
     // profiling
     EventTimer* timer = nullptr;
+    // render targets (Engine::ensureRenderTargets, Engine.cpp:351-377)
+    void* render_block = nullptr;
+    uint32_t render_w = 0, render_h = 0;
+    mpb::RenderBuffers rb{};
+
+    int ensure_render_targets(uint32_t w, uint32_t h) {
+        if (render_block && w == render_w && h == render_h) return MP_OK;
+        if (render_block) cudaFree(render_block);
+        render_block = nullptr;
+        const size_t px = size_t(w) * h, plane = (px * 4 + 255) & ~size_t(255);
+        MP_CUDA(cudaMalloc(&render_block, 4 * plane + 4 * plane));
+        char* p = static_cast<char*>(render_block);
+        rb.depth = reinterpret_cast<uint32_t*>(p);
+        rb.thick = reinterpret_cast<float*>(p + plane);
+        rb.smoothed = reinterpret_cast<float*>(p + 2 * plane);
+        rb.ndc = reinterpret_cast<float*>(p + 3 * plane);
+        rb.rgba = reinterpret_cast<float4*>(p + 4 * plane);
+        render_w = w;
+        render_h = h;
+        return MP_OK;
+    }
 
     void drop_graph() {
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -410,6 +432,7 @@ struct mp_engine {
         free_particles();
         free_cells();
         if (small_block) cudaFree(small_block);
+        if (render_block) cudaFree(render_block);
     }
 
     int alloc_particles(uint32_t count) {
@@ -864,6 +887,37 @@ int mp_engine_apply_mouse_pulse(mp_engine* e, const float ray_origin[3], const f
     c.falloff = e->params.mouse_falloff;
     const cudaError_t err = mpb::launch_mouse_pulse(c, e->d.vel, e->d.pos, static_cast<cudaStream_t>(stream));
     if (err != cudaSuccess) return fail(MP_ERR_CUDA, "mouse pulse launch: %s", cudaGetErrorString(err));
+    return MP_OK;
+}
+
+int mp_engine_render(mp_engine* e, const mp_render_params* rp, float* rgba, mp_stream stream) {
+    if (!e || !rp) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    mpb::RenderConsts c;
+    int rc = mpb::make_render_consts(*rp, e->params, e->n, e->scene == MP_SCENE_SPHERE_DROP, c);
+    if (rc != MP_OK) return rc;
+    DeviceGuard g(e->device);
+    rc = e->ensure_render_targets(rp->width, rp->height);
+    if (rc != MP_OK) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const cudaError_t err = mpb::launch_render(c, e->rb, e->d.pos, e->d.foam, e->d.sphere, s);
+    if (err != cudaSuccess) return fail(MP_ERR_CUDA, "render launch: %s", cudaGetErrorString(err));
+    if (rgba)
+        MP_CUDA(cudaMemcpyAsync(rgba, e->rb.rgba, size_t(rp->width) * rp->height * 16, cudaMemcpyDeviceToDevice, s));
+    return MP_OK;
+}
+
+int mp_engine_render_buffer(mp_engine* e, uint32_t which, void** dptr, size_t* bytes) {
+    if (!e || !dptr || !bytes) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!e->render_block) return fail(MP_ERR_INVALID_ARGUMENT, "nothing rendered yet");
+    const size_t px = size_t(e->render_w) * e->render_h;
+    switch (which) {
+        case MP_RENDER_BUF_COLOR: *dptr = e->rb.rgba; *bytes = 16 * px; break;
+        case MP_RENDER_BUF_DEPTH: *dptr = e->rb.depth; *bytes = 4 * px; break;
+        case MP_RENDER_BUF_SMOOTHED: *dptr = e->rb.smoothed; *bytes = 4 * px; break;
+        case MP_RENDER_BUF_THICKNESS: *dptr = e->rb.thick; *bytes = 4 * px; break;
+        case MP_RENDER_BUF_NDC_DEPTH: *dptr = e->rb.ndc; *bytes = 4 * px; break;
+        default: return fail(MP_ERR_INVALID_ARGUMENT, "unknown render buffer %u", which);
+    }
     return MP_OK;
 }
 

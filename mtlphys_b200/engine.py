@@ -266,6 +266,32 @@ class Engine:
                                                     C.c_float(radius), stream_handle(stream)),
               "mp_engine_apply_mouse_pulse")
 
+    # ---- headless rendering ----
+    def render(self, params=None, stream=None, **kw):
+        """Engine::render into a device image: (H, W, 4) float32 torch tensor
+        of linear RGBA in [0, 1], y = 0 on the top row.  params: a
+        RenderParams (default: _abi.default_render_params(**kw))."""
+        import torch
+
+        rp = params if params is not None else _abi.default_render_params(**kw)
+        out = torch.empty((rp.height, rp.width, 4), dtype=torch.float32, device=f"cuda:{self.device}")
+        check(self._lib.mp_engine_render(self._h, C.byref(rp), C.c_void_p(out.data_ptr()),
+                                         stream_handle(stream)), "mp_engine_render")
+        return out
+
+    def render_buffer(self, which: int):
+        """Zero-copy torch view of an image buffer of the last render (MP_RENDER_BUF_*)."""
+        import torch
+
+        p, nb = C.c_void_p(), C.c_size_t()
+        check(self._lib.mp_engine_render_buffer(self._h, which, C.byref(p), C.byref(nb)),
+              "mp_engine_render_buffer")
+        shape = (nb.value // 16, 4) if which == _abi.MP_RENDER_BUF_COLOR else (nb.value // 4,)
+        typestr = "<u4" if which == _abi.MP_RENDER_BUF_DEPTH else "<f4"
+        t = torch.as_tensor(_CudaArray(int(p.value), shape, "<f4" if typestr == "<f4" else "<i4", self),
+                            device=f"cuda:{self.device}")
+        return t.view(torch.float32) if which == _abi.MP_RENDER_BUF_DEPTH else t
+
     # ---- state snapshots ----
     def snapshot_bytes(self) -> bytes:
         """The engine state as a snapshot byte string (waits for queued work)."""

@@ -1,0 +1,113 @@
+"""Headless rendering (Engine.render) against the numpy restatement of the
+reference's render shaders (oracle/render_ref.py).
+
+Coverage and depth are bit-exact (the geometry runs with the same rounding
+in both); thickness, smoothing and shading go through exp / pow, whose CUDA
+and numpy results differ by a few ulps, hence tolerances there."""
+import numpy as np
+import pytest
+
+from mtlphys_b200 import Engine, _abi, configs
+from oracle import render_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def scene_engine(scene, n, steps):
+    p = _abi.default_params()
+    e = Engine(0)
+    e.set_params(p)
+    e.reset(n, scene)
+    for _ in range(steps):
+        e.step(1.0 / 120.0)
+    e.check_errors()
+    return e, p
+
+
+def oracle_render(e, p, rp, flags):
+    v, pr = _abi.render_camera(rp)
+    cam = R.Camera(rp, v, pr, p.bounds_min[:], p.bounds_max[:])
+    pos = e.positions()
+    foam = e.read(_abi.MP_BUF_FOAM)
+    sphere = e.sphere() if e.current_scene() == _abi.MP_SCENE_SPHERE_DROP else None
+    return R.render(cam, pos, foam, sphere, flags)
+
+
+def compare(e, want, rp, min_fluid=500):
+    n = rp.width * rp.height
+    depth = e.render_buffer(_abi.MP_RENDER_BUF_DEPTH).cpu().numpy()[:n].reshape(rp.height, rp.width)
+    depth = np.where(depth > 1e30, 0, depth)
+    np.testing.assert_array_equal(depth, want["depth"])
+    assert (want["depth"] > 0).sum() > min_fluid  # the case covers fluid
+    th = e.render_buffer(_abi.MP_RENDER_BUF_THICKNESS).cpu().numpy()[:n].reshape(rp.height, rp.width)
+    np.testing.assert_allclose(th, want["thickness"], rtol=1e-5, atol=1e-7)
+    sm = e.render_buffer(_abi.MP_RENDER_BUF_SMOOTHED).cpu().numpy()[:n].reshape(rp.height, rp.width)
+    np.testing.assert_allclose(sm, want["smoothed"], rtol=1e-5, atol=0)
+    ndc = e.render_buffer(_abi.MP_RENDER_BUF_NDC_DEPTH).cpu().numpy()[:n].reshape(rp.height, rp.width)
+    np.testing.assert_allclose(ndc, want["ndc"], rtol=0, atol=1e-6)
+    img = e.render_buffer(_abi.MP_RENDER_BUF_COLOR).cpu().numpy()[:n].reshape(rp.height, rp.width, 4)
+    assert np.isfinite(img).all() and img.min() >= 0 and img.max() <= 1
+    diff = np.abs(img - want["rgba"]).max(-1)
+    # shading: a few ulps of pow/exp; the rare larger differences sit where a
+    # normal is ill-conditioned (silhouettes, single-pixel fluid)
+    assert np.median(diff) < 1e-6
+    assert (diff > 2e-3).mean() < 5e-3, (diff > 2e-3).mean()
+    return img
+
+
+@pytest.mark.parametrize("scene,n,steps", [(_abi.MP_SCENE_DAM_BREAK, 6000, 30),
+                                           (_abi.MP_SCENE_SPHERE_DROP, 6000, 20),
+                                           (_abi.MP_SCENE_CUBE_DROP, 4000, 40)])
+def test_render_matches_the_restated_shaders(cuda, scene, n, steps):
+    e, p = scene_engine(scene, n, steps)
+    rp = _abi.default_render_params(width=320, height=240)
+    rp.eye[:] = [4.0, 3.5, 5.0]
+    rp.target[:] = [0.0, 0.0, 0.0]
+    out = e.render(rp)
+    assert out.shape == (240, 320, 4)
+    want = oracle_render(e, p, rp, rp.flags)
+    img = compare(e, want, rp)
+    np.testing.assert_array_equal(out.cpu().numpy(), img)  # the returned copy is the buffer
+    e.close()
+
+
+def test_render_pass_switches_and_camera_errors(cuda):
+    e, p = scene_engine(_abi.MP_SCENE_CUBE_DROP, 3000, 5)
+    rp = _abi.default_render_params(width=128, height=96, flags=0)
+    rp.eye[:] = [3.0, 3.0, 3.0]
+    e.render(rp)
+    want = oracle_render(e, p, rp, 0)
+    compare(e, want, rp, min_fluid=100)
+    bad = _abi.default_render_params(width=0)
+    with pytest.raises(_abi.MPError):
+        e.render(bad)
+    bad = _abi.default_render_params()
+    bad.eye[:] = bad.target[:]
+    with pytest.raises(_abi.MPError):
+        e.render(bad)
+    e.close()
+
+
+def test_render_the_million_particle_dam_break(cuda, tmp_path):
+    import torch
+
+    from mtlphys_b200.render import write_png
+
+    w = configs.dam_break()
+    e = Engine(0)
+    e.set_params(w.params)
+    e.reset(w.n, w.scene, w.desc)
+    for _ in range(20):
+        e.step(w.dt)
+    rp = _abi.default_render_params(width=1280, height=720)
+    rp.eye[:] = [13.0, 7.0, 13.0]
+    rp.target[:] = [4.3, 2.0, 4.3]
+    img = e.render(rp)
+    torch.cuda.synchronize()
+    a = img.cpu().numpy()
+    assert np.isfinite(a).all()
+    fluid = (e.render_buffer(_abi.MP_RENDER_BUF_SMOOTHED) > 0).float().mean().item()
+    assert 0.02 < fluid < 0.9, fluid
+    write_png(str(tmp_path / "dam.png"), a)
+    assert (tmp_path / "dam.png").stat().st_size > 1000
+    e.close()
