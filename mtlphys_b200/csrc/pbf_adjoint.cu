@@ -223,7 +223,11 @@ __global__ void __launch_bounds__(kBlock) k_adj_pre(AdjArgs a, uint32_t it) {
 // (dbar_j and the j-side terms only for pairs in both lists; the j-side
 // terms of a one-way pair are added to j atomically), and the particle's
 // density sums for the lambda adjoint.
-__global__ void __launch_bounds__(kBlock) k_adj_delta(AdjArgs a, uint32_t it) {
+// The two pair sweeps are compiled for 4 resident blocks per SM (64
+// registers): left alone they take ~90 and run 13-16% slower.
+constexpr int kSweepMinBlocks = 4;
+
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_delta(AdjArgs a, uint32_t it) {
     const uint32_t m = blockIdx.x * kBlock + threadIdx.x;
     const bool active = m < a.n;
     uint32_t scene = 0;
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_lbar(AdjArgs a, uint32_t it) {
 //   pbar_i += sum_j (rhobar_i + rhobar_j) grad W_ij
 //             + H_ij (Gbar_i - Gbar_j + 2 (Qbar_i + Qbar_j) g_ij)
 // (j-side terms of one-way pairs added to j atomically).
-__global__ void __launch_bounds__(kBlock) k_adj_lambda(AdjArgs a, uint32_t it) {
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_lambda(AdjArgs a, uint32_t it) {
     const uint32_t m = blockIdx.x * kBlock + threadIdx.x;
     if (m >= a.n) return;
     const StepConsts& c = a.t.scenes[a.scene_of[m]].c;
