@@ -19,13 +19,18 @@ namespace {
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 
 // Resident 256-thread blocks per SM the solver kernels are compiled for
-// (caps registers at 65536 / (256 * N)).
-#ifndef MPB_SOLVER_MIN_BLOCKS
-#define MPB_SOLVER_MIN_BLOCKS 4
+// (caps registers at 65536 / (256 * N)): the lambda passes run best at 4 (64
+// registers), the delta passes, whose bodies are lighter, at 6 (40 registers,
+// a small spill) -- measured on the 1M-particle dam break.
+#ifndef MPB_LAMBDA_MIN_BLOCKS
+#define MPB_LAMBDA_MIN_BLOCKS 4
+#endif
+#ifndef MPB_DELTA_MIN_BLOCKS
+#define MPB_DELTA_MIN_BLOCKS 6
 #endif
 
 template <bool LAST>
-__global__ void __launch_bounds__(256, MPB_SOLVER_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, MPB_LAMBDA_MIN_BLOCKS)
 k_lambda_first(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
                uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
                const uint32_t* __restrict__ sidx, float* __restrict__ lambdas,
@@ -35,7 +40,7 @@ k_lambda_first(StepConsts c, const float4* __restrict__ cur, float4* __restrict_
 }
 
 template <bool LAST>
-__global__ void __launch_bounds__(256, MPB_SOLVER_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, MPB_LAMBDA_MIN_BLOCKS)
 k_lambda(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
          const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
          const uint32_t* __restrict__ sidx, float* __restrict__ lambdas, RowMasks rm) {
@@ -44,7 +49,7 @@ k_lambda(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
 }
 
 template <bool LAST>
-__global__ void __launch_bounds__(256, MPB_SOLVER_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, MPB_DELTA_MIN_BLOCKS)
 k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
         const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
         const uint32_t* __restrict__ sidx, const SphereState* __restrict__ sphere,
