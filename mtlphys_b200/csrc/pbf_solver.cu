@@ -18,10 +18,15 @@ namespace {
 
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 
-// Resident 256-thread blocks per SM the solver kernels are compiled for
-// (caps registers at 65536 / (256 * N)): the lambda passes run best at 4 (64
-// registers), the delta passes, whose bodies are lighter, at 6 (40 registers,
-// a small spill) -- measured on the 1M-particle dam break.
+// Launch shape of the solver kernels, measured on the 1M-particle dam break:
+// blocks of 128 threads (slightly ahead of 256 and 512), and a residency
+// target that caps registers at 65536 / (256 * N) -- the lambda passes run
+// best with N = 4 (64 registers), the delta passes, whose bodies are
+// lighter, with N = 6 (40 registers, a small spill).
+#ifndef MPB_SOLVER_BLOCK
+#define MPB_SOLVER_BLOCK 128
+#endif
+constexpr uint32_t kSB = MPB_SOLVER_BLOCK;
 #ifndef MPB_LAMBDA_MIN_BLOCKS
 #define MPB_LAMBDA_MIN_BLOCKS 4
 #endif
@@ -30,7 +35,7 @@ inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 #endif
 
 template <bool LAST>
-__global__ void __launch_bounds__(256, MPB_LAMBDA_MIN_BLOCKS)
+__global__ void __launch_bounds__(kSB, MPB_LAMBDA_MIN_BLOCKS * 256 / kSB)
 k_lambda_first(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
                uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
                const uint32_t* __restrict__ sidx, float* __restrict__ lambdas,
@@ -40,7 +45,7 @@ k_lambda_first(StepConsts c, const float4* __restrict__ cur, float4* __restrict_
 }
 
 template <bool LAST>
-__global__ void __launch_bounds__(256, MPB_LAMBDA_MIN_BLOCKS)
+__global__ void __launch_bounds__(kSB, MPB_LAMBDA_MIN_BLOCKS * 256 / kSB)
 k_lambda(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
          const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
          const uint32_t* __restrict__ sidx, float* __restrict__ lambdas, RowMasks rm) {
@@ -49,7 +54,7 @@ k_lambda(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
 }
 
 template <bool LAST>
-__global__ void __launch_bounds__(256, MPB_DELTA_MIN_BLOCKS)
+__global__ void __launch_bounds__(kSB, MPB_DELTA_MIN_BLOCKS * 256 / kSB)
 k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
         const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
         const uint32_t* __restrict__ sidx, const SphereState* __restrict__ sphere,
@@ -91,24 +96,24 @@ cudaError_t launch_solver(const StepConsts& c, const DevState& d, uint32_t itera
         const bool first = it == 0, last = it + 1 == iterations;
         tbegin(t, s);
         if (first && last)
-            k_lambda_first<true><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart,
+            k_lambda_first<true><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart,
                                                       d.sidx, d.lambdas, d.ncount, rm);
         else if (first)
-            k_lambda_first<false><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart,
+            k_lambda_first<false><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart,
                                                        d.sidx, d.lambdas, d.ncount, rm);
         else if (last)
-            k_lambda<true><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart, d.sidx,
+            k_lambda<true><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart, d.sidx,
                                                 d.lambdas, rm);
         else
-            k_lambda<false><<<grid, 256, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart, d.sidx,
+            k_lambda<false><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_a, d.sorted_b, d.scell, d.cstart, d.sidx,
                                                  d.lambdas, rm);
         tend(t, first ? "lambda_count" : "lambda", s);
         tbegin(t, s);
         if (last)
-            k_delta<true><<<grid, 256, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
+            k_delta<true><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
                                                d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
         else
-            k_delta<false><<<grid, 256, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
+            k_delta<false><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
                                                 d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
         tend(t, last ? "delta_finalize" : "delta", s);
     }
