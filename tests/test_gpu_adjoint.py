@@ -50,11 +50,24 @@ from test_adjoint_ref import CASES, scene  # noqa: E402
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_one_step_adjoint_matches_the_fp64_restatement(cuda, name):
+    one_step_check(name)
+
+
+@pytest.mark.parametrize("name,iterations", [("floor_friction", 0), ("floor_friction", 1),
+                                             ("sphere_push", 0), ("sphere_push", 1)])
+def test_one_step_adjoint_with_zero_and_one_solver_iterations(cuda, name, iterations):
+    """No solver pass (predict + finalize only) and a single one."""
+    one_step_check(name, iterations)
+
+
+def one_step_check(name, iterations=None):
     from oracle import adjoint_ref as A
 
     torch = _torch()
     kw, sphere = CASES[name]
     p, x, v = scene(**kw)
+    if iterations is not None:
+        p.solver_iterations = iterations
     n = len(x)
     d = configs.lattice((kw["side"],) * 3, kw["origin"], 1)
     sid = _abi.MP_SCENE_SPHERE_DROP if sphere is not None else _abi.MP_SCENE_CUBE_DROP
@@ -97,6 +110,8 @@ def test_one_step_adjoint_matches_the_fp64_restatement(cuda, name):
     # dL/dk, a sum over all pairs with cancellation, inherits a few times that.
     k_tol = 1e-3 if kw.get("k", 0.1) < 1e-3 else 5e-3
     assert abs(g[_abi.MP_GRAD_SCORR_K] - kb) <= k_tol * abs(kb)
+    if p.solver_iterations == 0:
+        assert g[_abi.MP_GRAD_SCORR_K] == 0.0
     if sphere is not None:
         # through this step's push and the kinematic advance before it
         sb = np.zeros(7)
@@ -348,6 +363,35 @@ def test_batched_scenes_get_their_single_scene_gradients(cuda):
         gv, gk = run([s])
         np.testing.assert_allclose(gv_all[offs[s]:offs[s + 1]], gv, rtol=0, atol=1e-6 * np.abs(gv).max())
         assert abs(gk_all[s] - gk[0]) <= 1e-9 * abs(gk[0])
+
+
+def test_empty_scene_in_a_differentiable_batch(cuda):
+    """A scene with no particles next to a real one: the rollout and its
+    gradient run, the empty scene's parameter gradients are zero and the
+    other scene gets its single-scene gradients."""
+    torch = _torch()
+    w = configs.diff_cube(side=8, steps=6)
+    p = cube_params()
+    dev = torch.device("cuda", 0)
+
+    def run(counts):
+        b = make_batch([p] * len(counts), [w.desc] * len(counts), counts)
+        n = b.particle_count()
+        g = torch.zeros((n, 4), device=dev)
+        g[:, 1] = 1.0
+        b.rollout_forward(w.steps, 4)
+        dp, dv, ds = b.rollout_backward(g, None)
+        assert b.check_errors() == 0
+        out = dv.cpu().numpy(), ds.cpu().numpy()
+        b.close()
+        return out
+
+    dv_pair, ds_pair = run([0, w.n])
+    dv_one, ds_one = run([w.n])
+    assert not ds_pair[0].any()
+    np.testing.assert_allclose(dv_pair, dv_one, rtol=0, atol=1e-6 * np.abs(dv_one).max())
+    assert abs(ds_pair[1, _abi.MP_GRAD_SCORR_K] - ds_one[0, _abi.MP_GRAD_SCORR_K]) <= 1e-9 * abs(
+        ds_one[0, _abi.MP_GRAD_SCORR_K])
 
 
 def test_backward_after_a_state_change_is_refused(cuda):
