@@ -122,17 +122,7 @@ __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
     return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
 }
 
-// ---- SPH kernels ------------------------------------------------------------
-
-__device__ __forceinline__ float pow_n(float x, uint32_t n) {
-    if (n == 4u) {
-        const float x2 = x * x;
-        return x2 * x2;
-    }
-    float r = 1.0f;
-    for (uint32_t e = 0; e < n; ++e) r *= x;
-    return r;
-}
+// ---- SPH helpers ------------------------------------------------------------
 
 __device__ __forceinline__ float smoothstep_f(float e0, float e1, float x) {
     float t = __fdiv_rn(__fsub_rn(x, e0), __fsub_rn(e1, e0));
