@@ -247,3 +247,35 @@ def test_dam_break_1m_reference_k_strict_parity(eng):
     errs = run_and_check(eng, with_reference_k(configs.dam_break()), {0, 20}, 21)
     assert max(errs) <= POS_TOL
     print("dam_break (k=1e-4) max |dpos|:", errs)
+
+
+@pytest.mark.parametrize("workload", ["dam_break", "cube_drop"])
+def test_full_length_runs_stay_valid(eng, workload):
+    """The configs' full runs (dam break 300 steps at 1M particles, cube drop
+    200 steps) under graph replay: no device error word, every position and
+    velocity finite, inside the box, speeds under the CFL cap, and at the end
+    the hash invariants of the reference's spatial tests hold."""
+    w = configs.WORKLOADS[workload]()
+    eng.set_params(w.params)
+    eng.reset(w.n, w.scene, w.desc)
+    eng.set_graph_mode(True)
+    for t in range(w.steps):
+        eng.step(w.dt)
+        if t % 50 == 49:
+            assert eng.check_errors() == 0, t
+    eng.set_graph_mode(False)
+    pos, vel = eng.positions(), eng.velocities()
+    assert np.isfinite(pos).all() and np.isfinite(vel).all()
+    lo, hi = np.array(w.params.bounds_min[:]), np.array(w.params.bounds_max[:])
+    assert (pos[:, :3] >= lo).all() and (pos[:, :3] <= hi).all()
+    vmax = w.params.vmax * w.params.h / w.dt
+    assert (np.linalg.norm(vel[:, :3], axis=1) <= vmax * (1 + 1e-5)).all()
+    eng.build_spatial_hash()
+    cs, si, hs = eng.cell_start(), eng.sorted_index(), eng.cell_hashes()
+    assert cs[0] == 0 and cs[-1] == w.n and (np.diff(cs.astype(np.int64)) >= 0).all()
+    assert np.array_equal(np.sort(si), np.arange(w.n, dtype=si.dtype))
+    # slots of a cell hold exactly that cell's particles, in increasing index
+    cell_of_slot = np.repeat(np.arange(len(cs) - 1), np.diff(cs.astype(np.int64)))
+    assert np.array_equal(hs[si], cell_of_slot)
+    same = cell_of_slot[1:] == cell_of_slot[:-1]
+    assert (si[1:][same] > si[:-1][same]).all()
