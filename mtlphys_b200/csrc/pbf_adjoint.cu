@@ -20,8 +20,8 @@
 //              (Engine.cpp:694-707), one thread per scene
 //
 // The pair sweeps walk exactly the pairs of the forward iteration: the row
-// masks its lambda pass recorded (or the same full sweep for particles whose
-// rows overflowed).  The reference's neighbour search makes those lists
+// masks its lambda pass recorded (long rows distance-tested past their first
+// 32 candidates, as the forward delta pass does).  The reference's neighbour search makes those lists
 // asymmetric once particles leave their predicted cells (j is in i's list iff
 // j's predicted cell is next to i's current cell), so each pair term of i's
 // list is delivered to j by j's own sweep when i is in j's list too (a test
@@ -296,11 +296,7 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_delta(AdjArgs a
         const uint32_t ms = a.mask_stride;
         const RowMasks rm{const_cast<uint32_t*>(a.t.masks) + size_t(it) * 9 * ms,
                           const_cast<uint32_t*>(a.t.overflow) + size_t(it) * ms, ms};
-        if (rm.overflow[m] == 0u)
-            masked_pairs(c, src, a.t.cstart, rm, m, l, ax, ay, az, cx, cy, cz, body);
-        else
-            sweep<true>(c, src, a.t.cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, m,
-                        static_cast<const RowMasks*>(nullptr), body);
+        masked_pairs(c, src, a.t.cstart, rm, m, l, ax, ay, az, cx, cy, cz, body);
         const float ir = c.inv_rho0;
         const float4 qb = a.qbar[m];
         a.qbar[m] = make_float4(qb.x + px * ir, qb.y + py * ir, qb.z + pz * ir, 0.0f);
@@ -380,11 +376,7 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_lambda(AdjArgs 
     const uint32_t ms = a.mask_stride;
     const RowMasks rm{const_cast<uint32_t*>(a.t.masks) + size_t(it) * 9 * ms,
                       const_cast<uint32_t*>(a.t.overflow) + size_t(it) * ms, ms};
-    if (rm.overflow[m] == 0u)
-        masked_pairs(c, src, a.t.cstart, rm, m, l, ax, ay, az, cx, cy, cz, body);
-    else
-        sweep<true>(c, src, a.t.cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, m,
-                    static_cast<const RowMasks*>(nullptr), body);
+    masked_pairs(c, src, a.t.cstart, rm, m, l, ax, ay, az, cx, cy, cz, body);
     a.pbar[m] = make_float4(px, py, pz, 0.0f);
 }
 

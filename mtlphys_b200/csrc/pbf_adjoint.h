@@ -29,7 +29,7 @@ struct AdjStep {
     const float4* lam;            // iterations x stride: (l, lambda)
     const float4* delta;          // iterations x stride: unclamped corrections
     const uint32_t* masks;        // iterations x 9 x mask_stride row masks
-    const uint32_t* overflow;     // iterations x mask_stride
+    const uint32_t* overflow;     // iterations x mask_stride: bit r set for a long row r
 };
 
 struct AdjArgs {

@@ -28,7 +28,7 @@ struct BatchRecord {
     float4* lam;           // iterations x stride: (l, lambda) written by each lambda pass
     float4* delta;         // iterations x stride: unclamped correction of each delta pass
     uint32_t* masks;       // iterations x 9 x mask_stride: row masks of each lambda pass
-    uint32_t* overflow;    // iterations x mask_stride
+    uint32_t* overflow;    // iterations x mask_stride: bit r set for a long row r
     uint32_t stride;       // slots per lam / delta array
 };
 

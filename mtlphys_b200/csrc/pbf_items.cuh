@@ -211,8 +211,9 @@ __device__ __forceinline__ void count_neighbors_item(const StepConsts& c, uint32
 // the same stencil, hence exactly the same in-range pairs, so it walks these
 // bits instead of sweeping the 27 cells again.  Row-major layout (row r of
 // slot s at r * stride + s): the warp's stores and loads of one row coalesce.
-// A particle with a row longer than 32 candidates gets overflow[s] = 1 and is
-// swept in full by the delta pass.  rows == nullptr disables the masks.
+// A row longer than 32 candidates keeps the bits of its first 32 and sets bit
+// r of overflow[s]; the delta pass distance-tests that row's remaining
+// candidates again.  rows == nullptr disables the masks.
 struct RowMasks {
     uint32_t* rows;
     uint32_t* overflow;
@@ -289,10 +290,10 @@ __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float l
 // ANCHORED = true:  (px, py, pz) is the offset l from the anchor of hash cell
 // (pcx, pcy, pcz); r = ((A_i - A_cell(k)) + l_i) - l_k, A_i - A_cell(k) exact.
 //
-// With masks, every row of the stencil stores its bits (the particle's own
-// bit cleared) for the delta pass; a row longer than one chunk sets the
-// overflow flag.  Returns the number of in-range candidates, the particle
-// itself included.
+// With masks, every row of the stencil stores the bits of its first chunk (the
+// particle's own bit cleared) for the delta pass, and a row longer than one
+// chunk sets its bit in the overflow word.  Returns the number of in-range
+// candidates, the particle itself included.
 template <bool ANCHORED, class Body>
 __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __restrict__ src,
                                           const uint32_t* __restrict__ cstart, int cx, int cy, int cz,
@@ -352,14 +353,12 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
                 }
             }
             if (masks) {
-                // every row of the stencil is stored, empty ones as 0
-                if (b3 - b0 <= 32u) {
-                    const uint32_t self = s - b0;
-                    masks->rows[uint32_t((z - z0) * 3 + (y - y0)) * masks->stride + s] =
-                        self < 32u ? (first & ~(1u << self)) : first;
-                } else {
-                    over = 1;
-                }
+                // every row of the stencil is stored, empty ones as 0; a long
+                // row stores its first 32 candidates and flags the rest
+                const uint32_t row = uint32_t((z - z0) * 3 + (y - y0));
+                const uint32_t self = s - b0;
+                masks->rows[row * masks->stride + s] = self < 32u ? (first & ~(1u << self)) : first;
+                if (b3 - b0 > 32u) over |= 1u << row;
             }
         }
     }
@@ -476,11 +475,12 @@ __device__ __forceinline__ void finalize_particle(const StepConsts& c, uint32_t 
     if (!(isfinite(X + Y + Z) && isfinite(vx + vy + vz))) atomicOr(err, kDevErrNaN);
 }
 
-// The in-range pairs a lambda pass recorded in its row masks (rows of at most
-// 32 candidates; the particle's own bit cleared), walked with the anchored
-// neighbour vector of sweep<true>: body(k, q, rx, ry, rz, r2) for each.
-// (cx, cy, cz): the stencil cell of the particle at offset l from anchor
-// (ax, ay, az).
+// The in-range pairs a lambda pass recorded in its row masks (the particle's
+// own bit cleared), walked with the anchored neighbour vector of sweep<true>:
+// body(k, q, rx, ry, rz, r2) for each, in sweep<true>'s order (rows in
+// stencil order, slots ascending).  The candidates of a long row past its
+// first 32 are distance-tested again.  (cx, cy, cz): the stencil cell of the
+// particle at offset l from anchor (ax, ay, az).
 template <class Body>
 __device__ __forceinline__ void masked_pairs(const StepConsts& c, const float4* __restrict__ src,
                                              const uint32_t* __restrict__ cstart, const RowMasks& rm,
@@ -491,14 +491,17 @@ __device__ __forceinline__ void masked_pairs(const StepConsts& c, const float4* 
     const int z0 = max(cz - 1, 0), z1 = min(cz + 1, c.g.gz - 1);
     const int nx = x1 - x0 + 1;
     if (nx <= 0) return;
+    const uint32_t longrows = rm.overflow[s];
     const float ox0 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0)), l.x);
     const float ox1 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 1)), l.x);
     const float ox2 = __fadd_rn(__fsub_rn(ax, anchor_x(c.g, x0 + 2)), l.x);
     for (int z = z0; z <= z1; ++z) {
         const float oz = __fadd_rn(__fsub_rn(az, anchor_z(c.g, z)), l.z);
         for (int y = y0; y <= y1; ++y) {
-            uint32_t mask = rm.rows[uint32_t((z - z0) * 3 + (y - y0)) * rm.stride + s];
-            if (mask == 0u) continue;
+            const uint32_t row = uint32_t((z - z0) * 3 + (y - y0));
+            uint32_t mask = rm.rows[row * rm.stride + s];
+            const bool long_row = (longrows >> row) & 1u;
+            if (mask == 0u && !long_row) continue;
             const float oy = __fadd_rn(__fsub_rn(ay, anchor_y(c.g, y)), l.y);
             const uint32_t base = cell_hash(c.g, x0, y, z);
             const uint32_t b0 = cstart[base], b1 = cstart[base + 1];
@@ -511,6 +514,17 @@ __device__ __forceinline__ void masked_pairs(const StepConsts& c, const float4* 
                 const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y);
                 const float rz = __fsub_rn(oz, q.z);
                 body(k, q, rx, ry, rz, dist2(rx, ry, rz));
+            }
+            if (long_row) {
+                const uint32_t b3 = nx > 2 ? cstart[base + 3] : b2;
+                for (uint32_t k = b0 + 32u; k < b3; ++k) {
+                    const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
+                    const float4 q = __ldg(&src[k]);
+                    const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y);
+                    const float rz = __fsub_rn(oz, q.z);
+                    const float r2 = dist2(rx, ry, rz);
+                    if (r2 < c.h2) body(k, q, rx, ry, rz, r2);
+                }
             }
         }
     }
@@ -541,7 +555,11 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
     auto body = [&](uint32_t, const float4& q, float rx, float ry, float rz, float r2) {
         delta_add(c, l.w, q.w, rx, ry, rz, r2, dx, dy, dz);
     };
+#ifdef MPB_PARTICLE_OVERFLOW
     if (rm.rows != nullptr && rm.overflow[s] == 0u)
+#else
+    if (rm.rows != nullptr)
+#endif
         masked_pairs(c, src, cstart, rm, s, l, ax, ay, az, cx, cy, cz, body);
     else
         sweep<true>(c, src, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s,

@@ -22,7 +22,7 @@ struct DevState {
     uint32_t* sidx;         // sortedIndex: slot -> particle, stable within a cell
     uint32_t* scell;        // hash cell per sorted slot (anchor of the solver state)
     uint32_t* row_masks;            // 9 x mask_stride in-range bits per stencil row
-    uint32_t* mask_overflow;        // 1: a row exceeded 32 candidates (delta re-sweeps)
+    uint32_t* mask_overflow;        // bit r: row r exceeded 32 candidates (delta re-tests the rest)
     uint32_t mask_stride;
     uint32_t* ncount;       // neighbour count per particle
     float* lambdas;         // last lambda per particle
