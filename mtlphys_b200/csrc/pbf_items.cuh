@@ -17,9 +17,12 @@
 // Solver state (cell-anchored local coordinates): each particle's position is
 // A(c) + l, with c its hash cell (fixed for the step), A(c) = origin +
 // c * cellSize per axis in FP32 and l a small FP32 offset.  Neighbour vectors
-// are ((A_i - A_cell(k)) + l_i) - l_k with A_i - A_cell(k) exact, so they carry
-// ~1e-8 m of rounding instead of the ~5e-7 m of FP32 absolute coordinates at
-// 4-8 m, while each candidate is still one 16-byte load.  Box clamps, the
+// are ((A_i - A_cell(k)) + l_i) - l_k with A_i - A_cell(k) exact (Sterbenz:
+// neighbouring anchors of one sign are within a factor of two of each other,
+// except next to a zero coordinate, where the difference is off by at most
+// half an ulp of 0.1 m, ~4e-9 m), so they carry ~1e-8 m of rounding instead of
+// the ~5e-7 m of FP32 absolute coordinates at 4-8 m, while each candidate is
+// still one 16-byte load.  Box clamps, the
 // sphere push and finalize run in FP64 on A + l.  The first lambda pass runs
 // on the absolute FP32 predicted positions exactly as the reference does (so
 // the neighbour count it fuses in is bit-exact) and converts them to offsets,
@@ -387,8 +390,10 @@ __device__ __forceinline__ void lambda_first_item(const StepConsts& c, uint32_t 
                                       [&](uint32_t, const float4&, float rx, float ry, float rz,
                                           float r2) { acc.add(c, rx, ry, rz, r2); });
     const float lambda = acc.lambda(c);
-    // l = p - A(c): exact for the particle's own cell (Sterbenz), so the
-    // anchored state starts equal to the FP32 predicted position.
+    // l = p - A(c): exact for the particle's own cell (Sterbenz) unless the
+    // cell reaches a zero coordinate from below, where it rounds once, by at
+    // most half an ulp of the cell size; so the anchored state starts equal to
+    // the FP32 predicted position.
     nxt[s] = make_float4(__fsub_rn(p.x, anchor_x(c.g, cx)), __fsub_rn(p.y, anchor_y(c.g, cy)),
                          __fsub_rn(p.z, anchor_z(c.g, cz)), lambda);
     scell[s] = cell_local(c.g, cx, cy, cz);
