@@ -22,11 +22,11 @@
 // except next to a zero coordinate, where the difference is off by at most
 // half an ulp of 0.1 m, ~4e-9 m), so they carry ~1e-8 m of rounding instead of
 // the ~5e-7 m of FP32 absolute coordinates at 4-8 m, while each candidate is
-// still one 16-byte load.  Box clamps, the
-// sphere push and finalize run in FP64 on A + l.  The first lambda pass runs
-// on the absolute FP32 predicted positions exactly as the reference does (so
-// the neighbour count it fuses in is bit-exact) and converts them to offsets,
-// which is exact for the particle's own cell.
+// still one 16-byte load.  Box clamps, the sphere push and finalize run in
+// FP64 on A + l.  The first lambda pass runs on the absolute FP32 predicted
+// positions exactly as the reference does (so the neighbour count it fuses in
+// is bit-exact) and converts them to offsets, which is exact for the
+// particle's own cell.
 #pragma once
 
 #include "pbf_kernels.h"
