@@ -11,13 +11,15 @@ from oracle import oracle as O
 DT = 1.0 / 120.0
 
 
-def scene(side, origin, k=0.1, eps=100.0, jitter=0.01, vel=0.0, seed=1, sphere_radius=None):
+def scene(side, origin, k=0.1, eps=100.0, jitter=0.01, vel=0.0, seed=1, sphere_radius=None,
+          spacing=0.5):
     p = configs.base_params(3)
     p.scorr_k = k
     p.epsilon = eps
     if sphere_radius is not None:
         p.sphere_radius = sphere_radius
-    d = configs.lattice((side,) * 3, origin, seed, jitter=jitter * configs.H)
+    d = configs.lattice((side,) * 3, origin, seed, spacing=spacing * configs.H,
+                        jitter=jitter * configs.H)
     x = O.seed_scene(p, 0, side ** 3, d)[:, :3].astype(np.float64)
     v = np.random.default_rng(seed).normal(0.0, vel, size=x.shape)
     return p, x, v
@@ -31,6 +33,8 @@ CASES = {
     "sphere_push": (dict(side=6, origin=(2.0, 0.03, 2.0), vel=0.2, sphere_radius=0.12),
                     [2.12, 0.15, 2.12, 0.0, -1.0, 0.0, 0.12]),
     "gentle": (dict(side=6, origin=(2.0, 3.0, 2.0), k=1e-4, eps=1e4, vel=0.1), None),
+    # ~110 candidates per stencil row: rows longer than 32 candidates
+    "crowded": (dict(side=9, origin=(2.0, 3.0, 2.0), k=1e-4, eps=1e5, vel=0.1, spacing=0.3), None),
 }
 
 

@@ -220,6 +220,30 @@ def test_nan_input_sets_the_device_error_word(eng):
     assert eng.error_bits() == 0  # cleared
 
 
+@pytest.mark.parametrize("spacing,epsilon", [(0.35, 800.0), (0.22, 1e5)])
+def test_crowded_stencil_rows(eng, spacing, epsilon):
+    """A lattice packed at `spacing` h puts ~70 (0.35h) or ~250 (0.22h)
+    candidates in every stencil row: the lambda pass takes each row in
+    chunks of 32, and the delta pass walks the first chunk's recorded bits
+    and distance-tests the rest of the row.  Per step against the oracle
+    (epsilon raised for the denser lattice, where the default one makes the
+    step ill-conditioned and only the adaptive bound would apply)."""
+    p = _abi.default_params()
+    p.epsilon = epsilon
+    rng = np.random.default_rng(11)
+    side = int(round(3.0 / spacing))  # a cube of ~3h on a side
+    g = np.stack(np.meshgrid(*(np.arange(side),) * 3, indexing="ij"), -1).reshape(-1, 3)
+    pos = np.zeros((len(g), 4), np.float32)
+    pos[:, :3] = g * spacing * p.h + np.array([0.1, 1.0, 0.2]) + rng.uniform(-1e-2, 1e-2, g.shape) * p.h
+    pos[:, 3] = 1.0
+    vel = np.zeros_like(pos)
+    load_state(eng, pos, vel, p)
+    for _ in range(2):
+        pos, vel = eng.positions(), eng.velocities()
+        g = gpu_step(eng, 1.0 / 240.0)
+        compare_with_oracle(p, 1.0 / 240.0, pos, vel, g)
+
+
 def test_empty_engine_steps(eng):
     eng.set_params(_abi.default_params())
     eng.reset(0)
