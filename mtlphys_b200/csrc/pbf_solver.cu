@@ -21,8 +21,9 @@ inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 // Launch shape of the solver kernels, measured on the 1M-particle dam break:
 // blocks of 128 threads (slightly ahead of 256 and 512), and a residency
 // target that caps registers at 65536 / (256 * N) -- the lambda passes run
-// best with N = 4 (64 registers), the delta passes, whose bodies are
-// lighter, with N = 6 (40 registers, a small spill).
+// best with N = 4 (64 registers), the middle delta passes with N = 5 (48
+// registers), the last one, which also finalizes in FP64, with N = 6 (40
+// registers, a small spill).
 #ifndef MPB_SOLVER_BLOCK
 #define MPB_SOLVER_BLOCK 128
 #endif
@@ -32,6 +33,9 @@ constexpr uint32_t kSB = MPB_SOLVER_BLOCK;
 #endif
 #ifndef MPB_DELTA_MIN_BLOCKS
 #define MPB_DELTA_MIN_BLOCKS 6
+#endif
+#ifndef MPB_DELTA_MID_MIN_BLOCKS
+#define MPB_DELTA_MID_MIN_BLOCKS 5
 #endif
 
 template <bool LAST>
@@ -54,7 +58,7 @@ k_lambda(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
 }
 
 template <bool LAST>
-__global__ void __launch_bounds__(kSB, MPB_DELTA_MIN_BLOCKS * 256 / kSB)
+__global__ void __launch_bounds__(kSB, (LAST ? MPB_DELTA_MIN_BLOCKS : MPB_DELTA_MID_MIN_BLOCKS) * 256 / kSB)
 k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
         const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
         const uint32_t* __restrict__ sidx, const SphereState* __restrict__ sphere,
