@@ -225,7 +225,10 @@ __global__ void __launch_bounds__(kBlock) k_adj_pre(AdjArgs a, uint32_t it) {
 // density sums for the lambda adjoint.
 // The two pair sweeps are compiled for 4 resident blocks per SM (64
 // registers): left alone they take ~90 and run 13-16% slower.
-constexpr int kSweepMinBlocks = 4;
+#ifndef MPB_ADJ_SWEEP_MIN_BLOCKS
+#define MPB_ADJ_SWEEP_MIN_BLOCKS 4
+#endif
+constexpr int kSweepMinBlocks = MPB_ADJ_SWEEP_MIN_BLOCKS;
 
 __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_delta(AdjArgs a, uint32_t it) {
     const uint32_t m = blockIdx.x * kBlock + threadIdx.x;
