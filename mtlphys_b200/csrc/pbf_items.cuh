@@ -292,12 +292,15 @@ __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float l
 // ANCHORED = false: (px, py, pz) is the absolute FP32 position and r = p - q.
 // ANCHORED = true:  (px, py, pz) is the offset l from the anchor of hash cell
 // (pcx, pcy, pcz); r = ((A_i - A_cell(k)) + l_i) - l_k, A_i - A_cell(k) exact.
+// XW = true: each candidate carries the x anchor of its own hash cell in w
+// (the delta pass's output), so its x term is (A_i - q.w) + l_i, the same
+// value as the per-cell term the row would otherwise select by slot.
 //
 // With masks, every row of the stencil stores the bits of its first chunk (the
 // particle's own bit cleared) for the delta pass, and a row longer than one
 // chunk sets its bit in the overflow word.  Returns the number of in-range
 // candidates, the particle itself included.
-template <bool ANCHORED, class Body>
+template <bool ANCHORED, bool XW = false, class Body>
 __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __restrict__ src,
                                           const uint32_t* __restrict__ cstart, int cx, int cy, int cz,
                                           float px, float py, float pz, int pcx, int pcy, int pcz,
@@ -316,10 +319,15 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
         }
         return 0;
     }
+#ifndef MPB_NO_XW
+    constexpr bool kXW = ANCHORED && XW;
+#else
+    constexpr bool kXW = false;
+#endif
     float ox0 = px, ox1 = px, ox2 = px;
-    float aiy = 0.0f, aiz = 0.0f;
+    float aix = 0.0f, aiy = 0.0f, aiz = 0.0f;
     if (ANCHORED) {
-        const float aix = anchor_x(c.g, pcx);
+        aix = anchor_x(c.g, pcx);
         aiy = anchor_y(c.g, pcy);
         aiz = anchor_z(c.g, pcz);
         ox0 = __fadd_rn(__fsub_rn(aix, anchor_x(c.g, x0)), px);
@@ -339,8 +347,8 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
                 const uint32_t c1 = min(c0 + 32u, b3);
                 uint32_t mask = 0;
                 for (uint32_t k = c0; k < c1; ++k) {
-                    const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
                     const float4 q = __ldg(&src[k]);
+                    const float ox = kXW ? __fadd_rn(__fsub_rn(aix, q.w), px) : (k < b1 ? ox0 : (k < b2 ? ox1 : ox2));
                     const float r2 = dist2(__fsub_rn(ox, q.x), __fsub_rn(oy, q.y), __fsub_rn(oz, q.z));
                     mask |= uint32_t(r2 < c.h2) << (k - c0);
                 }
@@ -349,8 +357,8 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
                 while (mask) {
                     const uint32_t k = c0 + uint32_t(__ffs(mask) - 1);
                     mask &= mask - 1;
-                    const float ox = k < b1 ? ox0 : (k < b2 ? ox1 : ox2);
                     const float4 q = __ldg(&src[k]);
+                    const float ox = kXW ? __fadd_rn(__fsub_rn(aix, q.w), px) : (k < b1 ? ox0 : (k < b2 ? ox1 : ox2));
                     const float rx = __fsub_rn(ox, q.x), ry = __fsub_rn(oy, q.y), rz = __fsub_rn(oz, q.z);
                     body(k, q, rx, ry, rz, dist2(rx, ry, rz));
                 }
@@ -405,7 +413,8 @@ __device__ __forceinline__ void lambda_first_item(const StepConsts& c, uint32_t 
     if (LAST) lambdas[j] = lambda;
 }
 
-// Later lambda passes on the anchored state.
+// Later lambda passes on the anchored state: cur is the previous delta pass's
+// output, (l, x anchor of the hash cell) per slot.
 template <bool LAST>
 __device__ __forceinline__ void lambda_item(const StepConsts& c, uint32_t s,
                                             const float4* __restrict__ cur, float4* __restrict__ nxt,
@@ -419,7 +428,7 @@ __device__ __forceinline__ void lambda_item(const StepConsts& c, uint32_t s,
     cell_of(c.g, __fadd_rn(anchor_x(c.g, pcx), l.x), __fadd_rn(anchor_y(c.g, pcy), l.y),
             __fadd_rn(anchor_z(c.g, pcz), l.z), cx, cy, cz);
     LambdaAcc acc;
-    sweep<true>(c, cur, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s, rm.rows ? &rm : nullptr,
+    sweep<true, true>(c, cur, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s, rm.rows ? &rm : nullptr,
                 [&](uint32_t, const float4&, float rx, float ry, float rz, float r2) {
                     acc.add(c, rx, ry, rz, r2);
                 });
@@ -599,8 +608,10 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
         }
     }
     if (!LAST) {
+        // w: the x anchor of the particle's hash cell, for the next lambda
+        // pass's neighbour vectors
         dst[s] = make_float4(float(__dsub_rn(X, double(ax))), float(__dsub_rn(Y, double(ay))),
-                             float(__dsub_rn(Z, double(az))), 0.0f);
+                             float(__dsub_rn(Z, double(az))), ax);
         return;
     }
     finalize_particle(c, sidx[s], X, Y, Z, pos, vel, prev, ncount, foam, err);
