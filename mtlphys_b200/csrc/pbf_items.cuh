@@ -285,9 +285,9 @@ __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float l
 // (3 consecutive cells, one contiguous slot range) is taken in chunks of 32
 // candidates: phase 1 loads every candidate once, does only the distance test
 // and sets a bit for each one within h; phase 2 visits just the set bits and
-// calls body(k, q, rx, ry, rz, r2) with k the candidate's slot.  The in-range body, about an eighth of the
-// candidates, then runs on most lanes of the warp instead of on the few lanes
-// whose candidate happened to be in range.
+// calls body(k, q, rx, ry, rz, r2) with k the candidate's slot.  The in-range
+// body, about an eighth of the candidates, then runs on most lanes of the warp
+// instead of on the few lanes whose candidate happened to be in range.
 //
 // ANCHORED = false: (px, py, pz) is the absolute FP32 position and r = p - q.
 // ANCHORED = true:  (px, py, pz) is the offset l from the anchor of hash cell
