@@ -229,10 +229,18 @@ struct RowMasks {
 // functions (the single-scene kernels, the persistent batch kernel) rounds
 // identically and gives bit-identical results.
 
-// Density / gradient terms of one in-range candidate at offset r, r2 = |r|^2
-// < h^2 (Constraints.metal:112-118).  The particle itself (r2 = 0) adds W(0).
+// densityLambdaSorted's sums for one particle (Constraints.metal:99-121): the
+// density starts at the particle's own W(0) whether or not its slot lies in
+// the stencil of its current cell (a particle can drift two cells from its
+// hash cell within a step), and add() takes the terms of every other
+// in-range candidate at offset r, r2 = |r|^2 < h^2, in slot order.  A
+// candidate at the particle's own position (r2 = 0) adds W(0) and no gradient.
 struct LambdaAcc {
     float dens = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f, gsq = 0.0f;
+    // the particle's own W(0)
+    __device__ __forceinline__ void self(const StepConsts& c) {
+        dens = __fmul_rn(__fmul_rn(__fmul_rn(c.poly6, c.h2), c.h2), c.h2);
+    }
     __device__ __forceinline__ void add(const StepConsts& c, float rx, float ry, float rz, float r2) {
         const float d = __fsub_rn(c.h2, r2);
         dens = __fmaf_rn(__fmul_rn(__fmul_rn(c.poly6, d), d), d, dens);
@@ -405,10 +413,13 @@ __device__ __forceinline__ void lambda_first_item(const StepConsts& c, uint32_t 
     int cx, cy, cz;
     cell_of(c.g, p.x, p.y, p.z, cx, cy, cz);
     LambdaAcc acc;
+    acc.self(c);
     const uint32_t cnt = sweep<false>(c, cur, cstart, cx, cy, cz, p.x, p.y, p.z, cx, cy, cz, s,
                                       rm.rows ? &rm : nullptr,
-                                      [&](uint32_t, const float4&, float rx, float ry, float rz,
-                                          float r2) { acc.add(c, rx, ry, rz, r2); });
+                                      [&](uint32_t k, const float4&, float rx, float ry, float rz,
+                                          float r2) {
+                                          if (k != s) acc.add(c, rx, ry, rz, r2);
+                                      });
     const float lambda = acc.lambda(c);
     // l = p - A(c): exact for the particle's own cell (Sterbenz) unless the
     // cell reaches a zero coordinate from below, where it rounds once, by at
@@ -440,10 +451,11 @@ __device__ __forceinline__ void lambda_item(const StepConsts& c, uint32_t s,
     cell_of(c.g, __fadd_rn(anchor_x(c.g, pcx), l.x), __fadd_rn(anchor_y(c.g, pcy), l.y),
             __fadd_rn(anchor_z(c.g, pcz), l.z), cx, cy, cz);
     LambdaAcc acc;
+    acc.self(c);
     sweep<true, true>(c, cur, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s, rm.rows ? &rm : nullptr,
-                [&](uint32_t, const float4&, float rx, float ry, float rz, float r2) {
-                    acc.add(c, rx, ry, rz, r2);
-                });
+                      [&](uint32_t k, const float4&, float rx, float ry, float rz, float r2) {
+                          if (k != s) acc.add(c, rx, ry, rz, r2);
+                      });
     const float lambda = acc.lambda(c);
     nxt[s] = make_float4(l.x, l.y, l.z, lambda);
     if (LAST) lambdas[sidx[s]] = lambda;

@@ -86,3 +86,25 @@ def position_tolerance(p, dt: float, pos4, vel4, sphere=None) -> float:
     it by less than that); otherwise 4x the measured sensitivity."""
     kappa = sensitivity(p, dt, pos4, vel4, sphere)
     return POS_TOL if kappa <= POS_TOL else 4.0 * kappa
+
+
+def random_scene(seed: int, n: int):
+    """A seeded random cloud in the reference's default box ([-3, 3] x [-3, 6]
+    x [-3, 3]): 60% uniform in a 1 m cube, 30% in three tight clumps (cells of
+    dozens to hundreds of particles: long stencil rows and long cell
+    segments), 10% anywhere in a slightly larger box (positions outside the
+    grid, clamped by the hash); velocities N(0, 0.5 m/s).  Returns float32
+    (n, 4) positions (w = 1) and velocities (w = 0)."""
+    rng = np.random.default_rng(seed)
+    n_u, n_c = int(0.6 * n), int(0.3 * n)
+    n_o = n - n_u - n_c
+    u = rng.uniform(-0.5, 0.5, (n_u, 3)) + np.array([0.0, 1.0, 0.0])
+    centres = rng.uniform(-0.4, 0.4, (3, 3)) + np.array([0.0, 1.0, 0.0])
+    cl = centres[rng.integers(0, 3, n_c)] + rng.normal(0.0, 0.03, (n_c, 3))
+    o = rng.uniform([-3.2, -3.2, -3.2], [3.2, 6.2, 3.2], (n_o, 3))
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = np.concatenate([u, cl, o])
+    pos[:, 3] = 1.0
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0.0, 0.5, (n, 3))
+    return pos, vel

@@ -10,7 +10,7 @@ import pytest
 from mtlphys_b200 import _abi, configs
 from oracle import oracle as O
 from parity import (H, POS_TOL, assert_equal_u32, assert_lambdas, assert_positions,
-                    assert_velocities, golden, position_tolerance)
+                    assert_velocities, golden, position_tolerance, random_scene)
 
 G = golden()
 
@@ -184,6 +184,27 @@ def test_oracle_matches_reference_shaders_live_config_box():
         o = O.step(p, w.dt, pos, vel)
         assert_equal_u32(o["sorted_index"], r["sorted_index"], "sortedIndex")
         assert_positions(o["pos"], r["pos"])
+        pos, vel = r["pos"], r["vel"]
+
+
+@pytest.mark.skipif(not O.has_ref(), reason="reference sources not built here (oracle/_ref)")
+@pytest.mark.parametrize("seed,n", [(1, 600), (2, 2000), (3, 3000)])
+def test_oracle_matches_reference_shaders_random_clouds(seed, n):
+    """FP64 oracle vs the reference's shader code on seeded random clouds
+    (uniform, tight clumps, points outside the grid; random velocities), two
+    steps from each state: hash, cellStart, sortedIndex and neighbour counts
+    bit-exact, positions within the step's bound (1e-5 h, or 4x the measured
+    1-ulp sensitivity where the clumps make the step ill-conditioned)."""
+    p = ref_params()
+    dt = 1.0 / 240.0
+    pos, vel = random_scene(seed, n)
+    O.ref_set_threads(1)
+    for _ in range(2):
+        r = O.ref_step(p, dt, pos, vel)
+        o = O.step(p, dt, pos, vel)
+        for key in ("hashes", "cell_start", "sorted_index", "neighbor_counts"):
+            assert_equal_u32(o[key], r[key], key)
+        assert_positions(o["pos"], r["pos"], position_tolerance(p, dt, pos, vel))
         pos, vel = r["pos"], r["vel"]
 
 
