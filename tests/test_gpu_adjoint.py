@@ -124,6 +124,46 @@ def one_step_check(name, iterations=None):
     b.close()
 
 
+@pytest.mark.parametrize("seed", [1, 2])
+def test_one_step_adjoint_on_random_clouds(cuda, seed):
+    """One step of a seeded random cloud (tight clumps, points outside the
+    grid and clamped by the hash and the box, random velocities) at the
+    reference engine's parameters: the CUDA VJP equals the FP64 numpy VJP on
+    the same FP32 input state."""
+    from oracle import adjoint_ref as A
+    from parity import random_scene
+
+    torch = _torch()
+    p = _abi.default_params()
+    p.solver_iterations = 3
+    pos4, vel4 = random_scene(seed, 600)
+    n = len(pos4)
+    b = make_batch([p], None, [n], [_abi.MP_SCENE_CUBE_DROP])
+    dev = torch.device("cuda", 0)
+    pos0 = torch.tensor(pos4, device=dev)
+    vel0 = torch.tensor(vel4, device=dev)
+    b.tensor(_abi.MP_BUF_POSITIONS).copy_(pos0)
+    b.tensor(_abi.MP_BUF_VELOCITIES).copy_(vel0)
+    b.rollout_forward(1, 1)
+    rng = np.random.default_rng(seed + 10)
+    wx, wv = rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    gp = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    gv = torch.zeros_like(gp)
+    gp[:, :3] = torch.tensor(wx, dtype=torch.float32)
+    gv[:, :3] = torch.tensor(wv, dtype=torch.float32)
+    dp, dv, ds = b.rollout_backward(gp, gv)
+    torch.cuda.synchronize()
+    assert b.check_errors() == 0
+    c = A.consts(p, DT)
+    _, _, tape = A.forward(c, pos4[:, :3].astype(np.float64), vel4[:, :3].astype(np.float64), None)
+    xb, vb, kb, _, _ = A.adjoint(c, tape, wx, wv)
+    rel = lambda a, r: np.linalg.norm(a - r) / np.linalg.norm(r)
+    assert rel(dp[:, :3].double().cpu().numpy(), xb) < 1e-3
+    assert rel(dv[:, :3].double().cpu().numpy(), vb) < 1e-3
+    assert abs(ds.cpu().numpy()[0][_abi.MP_GRAD_SCORR_K] - kb) <= 1e-3 * abs(kb)
+    b.close()
+
+
 # ---- rollouts against finite differences of the FP64 oracle ------------------------
 
 def cube_params(cfm=1e4):
