@@ -261,6 +261,26 @@ def test_random_clouds(eng, seed, n):
         compare_with_oracle(p, 1.0 / 240.0, pos, vel, g)
 
 
+@pytest.mark.parametrize("seed", [5, 6])
+def test_random_clouds_with_sphere(eng, seed):
+    """A seeded random cloud with the kinematic sphere inside it (moving):
+    every iteration pushes the particles it overlaps out to its surface.  Two
+    steps against the oracle, sphere state included."""
+    p = _abi.default_params()
+    pos, vel = random_scene(seed, 2000)
+    load_state(eng, pos, vel, p, _abi.MP_SCENE_SPHERE_DROP)
+    rng = np.random.default_rng(seed)
+    eng.set_sphere((0.05, 1.0, -0.05), tuple(rng.normal(0.0, 1.0, 3)), 0.25)
+    for _ in range(2):
+        pos, vel, sph = eng.positions(), eng.velocities(), eng.sphere()
+        g = gpu_step(eng, 1.0 / 240.0)
+        compare_with_oracle(p, 1.0 / 240.0, pos, vel, g, sph)
+        s_gpu = eng.sphere()
+        s_or = np.array(sph, np.float64)
+        O.step(p, 1.0 / 240.0, pos, vel, s_or)
+        assert np.abs(s_gpu[:6] - s_or[:6]).max() < 1e-5
+
+
 def test_empty_engine_steps(eng):
     eng.set_params(_abi.default_params())
     eng.reset(0)
