@@ -33,7 +33,20 @@ def oracle_render(e, p, rp, flags):
     return R.render(cam, pos, foam, sphere, flags)
 
 
-def compare(e, want, rp, min_fluid=500):
+def silhouette(fluid):
+    """Pixels whose 3x3 neighbourhood holds both fluid and sky."""
+    pad = np.pad(fluid, 1, constant_values=False)
+    all_f = np.ones_like(fluid)
+    any_f = np.zeros_like(fluid)
+    for dy in range(3):
+        for dx in range(3):
+            w = pad[dy:dy + fluid.shape[0], dx:dx + fluid.shape[1]]
+            all_f &= w
+            any_f |= w
+    return any_f & ~all_f
+
+
+def compare(e, want, rp, min_fluid=500, whole_image=True):
     n = rp.width * rp.height
     depth = e.render_buffer(_abi.MP_RENDER_BUF_DEPTH).cpu().numpy()[:n].reshape(rp.height, rp.width)
     depth = np.where(depth > 1e30, 0, depth)
@@ -51,7 +64,10 @@ def compare(e, want, rp, min_fluid=500):
     # shading: a few ulps of pow/exp; the rare larger differences sit where a
     # normal is ill-conditioned (silhouettes, single-pixel fluid)
     assert np.median(diff) < 1e-6
-    assert (diff > 2e-3).mean() < 5e-3, (diff > 2e-3).mean()
+    bad = diff > 2e-3
+    assert (bad & ~silhouette(want["smoothed"] > 0)).mean() < 5e-3
+    if whole_image:
+        assert bad.mean() < 5e-3, bad.mean()
     return img
 
 
@@ -110,4 +126,33 @@ def test_render_the_million_particle_dam_break(cuda, tmp_path):
     assert 0.02 < fluid < 0.9, fluid
     write_png(str(tmp_path / "dam.png"), a)
     assert (tmp_path / "dam.png").stat().st_size > 1000
+    e.close()
+
+
+@pytest.mark.parametrize("eye", [(0.3, 1.2, 0.9), (4.0, 3.0, 5.0)])
+def test_render_random_cloud(cuda, eye):
+    """A seeded random cloud after one step, seen from inside it (particles
+    behind the camera and across the near plane) and from outside the box
+    (clumps, stragglers far from the fluid): coverage and depth bit-exact
+    against the restated shaders, shading within the usual tolerances off
+    silhouettes.  Seen from outside, the stragglers make silhouettes a tenth
+    of the image, and there the reconstructed normal is ill-conditioned, so
+    the whole-image bound does not apply."""
+    from parity import random_scene
+
+    p = _abi.default_params()
+    pos, vel = random_scene(1, 8000)
+    e = Engine(0)
+    e.set_params(p)
+    e.reset(len(pos))
+    e.write(_abi.MP_BUF_POSITIONS, pos)
+    e.write(_abi.MP_BUF_VELOCITIES, vel)
+    e.step(1.0 / 240.0)
+    e.check_errors()
+    rp = _abi.default_render_params(width=256, height=192)
+    rp.eye[:] = list(eye)
+    rp.target[:] = [0.0, 1.0, 0.0]
+    e.render(rp)
+    want = oracle_render(e, p, rp, rp.flags)
+    compare(e, want, rp, min_fluid=200, whole_image=False)
     e.close()
