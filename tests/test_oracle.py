@@ -208,6 +208,31 @@ def test_oracle_matches_reference_shaders_random_clouds(seed, n):
         pos, vel = r["pos"], r["vel"]
 
 
+@pytest.mark.skipif(not O.has_ref(), reason="reference sources not built here (oracle/_ref)")
+@pytest.mark.parametrize("seed", [5, 6])
+def test_oracle_matches_reference_shaders_random_cloud_with_sphere(seed):
+    """The same random clouds with the moving sphere inside them: the
+    oracle's sphere kinematics and per-iteration push against the reference's
+    (host kinematics restated by the harness, sphereCollision compiled from
+    its shader), two steps."""
+    p = ref_params()
+    dt = 1.0 / 240.0
+    pos, vel = random_scene(seed, 2000)
+    rng = np.random.default_rng(seed)
+    sph_r = np.array([0.05, 1.0, -0.05, *rng.normal(0.0, 1.0, 3), 0.25], np.float32)
+    sph_o = sph_r.astype(np.float64)
+    O.ref_set_threads(1)
+    for _ in range(2):
+        tol = position_tolerance(p, dt, pos, vel, sph_o.copy())
+        o = O.step(p, dt, pos, vel, sph_o)
+        r = O.ref_step(p, dt, pos, vel, sph_r)
+        for key in ("hashes", "cell_start", "sorted_index", "neighbor_counts"):
+            assert_equal_u32(o[key], r[key], key)
+        assert_positions(o["pos"], r["pos"], tol)
+        assert np.abs(sph_o[:6] - sph_r[:6]).max() < 1e-5
+        pos, vel = r["pos"], r["vel"]
+
+
 def test_integrate_matches_the_reference_shader():
     """Engine::integrate restated in FP32 equals the reference's Integrate.metal
     (compiled as C++) bit for bit, including box clamps and reflections."""
