@@ -82,57 +82,93 @@ REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_powe
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+    """SM clock and clock-event reasons of one GPU, sampled every few
+    milliseconds through NVML by a thread while the timed region runs (a
+    1M-particle timed region lasts tens of milliseconds, so nvidia-smi's
+    200 ms loop would see at most one sample); nvidia-smi is the fallback."""
 
-    def __init__(self, gpu_id: str):
-        self.gpu_id = gpu_id
-        self.proc = None
-        self.lines: list[str] = []
+    PERIOD_S = 0.004
 
-    def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except Exception:
-            self.proc = None
-        return self
+    def __init__(self, gpu_uuid: str):
+        self.uuid = gpu_uuid
+        self.samples: list[tuple[float, float, set]] = []
+        self.source = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+    def _nvml_loop(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self._stop.is_set():
             try:
-                self.proc.wait(timeout=5)
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((sm, mx, {k for k, b in bits.items() if r & b}))
             except Exception:
-                self.proc.kill()
+                pass
+            self._stop.wait(self.PERIOD_S)
 
-    def summary(self) -> dict:
-        sm, mx, reasons = [], [], set()
-        for line in self.lines:
+    def _smi_loop(self):
+        for line in self._proc.stdout:
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 8:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
+                sm, mx = float(parts[0]), float(parts[1])
             except ValueError:
                 continue
-            for name, val in zip(REASONS, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+            self.samples.append((sm, mx, {k for k, v in zip(REASONS, parts[4:8])
+                                          if v.lower().startswith("active")}))
+
+    def __enter__(self):
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByUUID(self.uuid)
+            self._thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.source = "nvml"
+        except Exception:
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                self._proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", self.uuid, f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                     "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._thread = threading.Thread(target=self._smi_loop, daemon=True)
+                self.source = "nvidia-smi"
+            except Exception:
+                self._thread = None
+        if self._thread is not None:
+            self._thread.start()
+            t0 = time.perf_counter()  # the first sample lands before the timed region
+            while not self.samples and time.perf_counter() - t0 < 2.0:
+                time.sleep(0.001)
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": self.source}
+        reasons = set().union(*(r for _, _, r in self.samples))
+        return {"sm_mhz": statistics.median(s for s, _, _ in self.samples),
+                "sm_max_mhz": max(m for _, m, _ in self.samples), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": self.source}
 
 
 # ---- distributed plumbing ----------------------------------------------------------
@@ -339,10 +375,8 @@ def run_ours(args, world, rank, local) -> dict | None:
         "metric": METRIC, "value": round(value, 5), "unit": "ms/step", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: seeded jittered lattice (dam break), no dataset",
-        "config": {**w.describe(), "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "flushed between timed steps (256 MiB write outside the events)",
-                   "mode": "CUDA graph replay of the step"},
+        "data": f"synthetic: seeded jittered lattice ({w.name}), no dataset",
+        "config": bench_config(w, world), "mode": "CUDA graph replay of the step",
         "ms_per_step_hot_l2": round(hot_ms, 5),
         "steps_per_s": round(1000.0 / ms_per_step, 2),
         "particle_steps_per_s": round(n * world * 1000.0 / ms_per_step, 1),
@@ -608,25 +642,43 @@ def cpu_baseline(w, args) -> dict:
 
 
 # ---- reference arm ----------------------------------------------------------------------
+L2_NOTE = "flushed between timed steps (256 MiB write outside the timed region)"
+
+
+def bench_config(w, world: int) -> dict:
+    """The `config` both arms print: the workload with its sizes, how the work
+    is spread, and how caches are flushed between timed steps."""
+    return {**w.describe(), "parallelism": "replicas" if world > 1 else "single", "l2": L2_NOTE}
+
+
 def run_reference(args, world, rank) -> dict | None:
+    """The reference's own CPU implementation of the step on the host cores:
+    its compute shaders (engine/shaders/*.metal) compiled as C++ into
+    oracle/_ref and dispatched in Engine::step order (engine/src/Engine.cpp:
+    685-811), OpenMP over all host cores; the FP64 oracle port where _ref was
+    not built.  Same workload, warm-up and timed steps as our arm; nothing of
+    the product package is imported or loaded (the workload comes from
+    oracle/params.py, which a CPU test pins to the product's).  The shaders
+    hard-code s_corr k = 1e-4 (Constraints.metal:158); the config says so."""
     if rank != 0:
         return None
     import numpy as np
 
-    from mtlphys_b200 import configs
     from oracle import oracle as O
+    from oracle import params as OP
 
-    w = configs.WORKLOADS[args.workload]()
+    w = OP.WORKLOADS[args.workload]()
     cores = os.cpu_count() or 1
     pos = O.seed_scene(w.params, w.scene, w.n, w.desc)
     vel = np.zeros_like(pos)
+    config = bench_config(w, world)
     if O.has_ref():
         kind = "reference"
         O.ref_set_threads(cores)
-        p = w.params.copy()
+        config["scorr_k"] = 1e-4
 
         def step(pos, vel):
-            o = O.ref_step(p, w.dt, pos, vel)
+            o = O.ref_step(w.params, w.dt, pos, vel)
             return o["pos"], o["vel"]
         what = ("the reference's compute shaders (engine/shaders/*.metal) compiled as C++, "
                 "dispatched in Engine::step order; s_corr k is the shaders' hard-coded 1e-4")
@@ -638,26 +690,95 @@ def run_reference(args, world, rank) -> dict | None:
             o = O.step(w.params, w.dt, pos, vel)
             return (np.concatenate([o["pos"], np.ones((w.n, 1))], axis=1).astype(np.float32),
                     np.concatenate([o["vel"], np.zeros((w.n, 1))], axis=1).astype(np.float32))
-        what = "FP64 oracle port"
-    for _ in range(min(args.warmup, 2)):
+        what = "FP64 oracle port (the reference's shaders were not compiled here)"
+    flush = np.empty(L2_FLUSH_BYTES, np.uint8)
+    for _ in range(args.warmup):
         pos, vel = step(pos, vel)
-    t0 = time.perf_counter()
-    steps = 0
-    while steps < args.steps and (steps == 0 or time.perf_counter() - t0 < args.cpu_budget_s):
+    total = 0.0
+    for i in range(args.steps):
+        flush.fill(i & 0xFF)  # evict the host caches, outside the timed region
+        t0 = time.perf_counter()
         pos, vel = step(pos, vel)
-        steps += 1
-    ms = (time.perf_counter() - t0) * 1000.0 / steps
+        total += time.perf_counter() - t0
+    ms = total * 1000.0 / args.steps
     return {
         "metric": METRIC, "value": round(ms, 3), "unit": "ms/step", "impl": "reference",
-        "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 2), "ms_per_step": round(ms, 3),
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: seeded jittered lattice (dam break), no dataset",
-        "config": {**w.describe(), "parallelism": "host cores (OpenMP)"},
+        "data": f"synthetic: seeded jittered lattice ({w.name}), no dataset",
+        "config": config,
         "cpu_baseline": {"value": round(ms, 3), "unit": "ms/step", "cores": cores, "kind": kind,
-                         "sample": f"{steps} steps of {w.name} ({w.n} particles): {what}"},
+                         "sample": f"{args.steps} whole steps of {w.name} ({w.n} particles) after "
+                                   f"{args.warmup} warm-up steps: {what}"},
         "e2e": {"value": round(ms, 3), "unit": "ms/step", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+
+
+# ---- fixed short runs for profilers ---------------------------------------------------
+def run_profile(which: str) -> str:
+    """One workload run once, a short fixed sequence of launches for a
+    profiler to capture: `step` (1M dam break, 3 steps), `batch` (256 cube
+    drops, 3 batched steps), `adjoint` (97K cube, 20-step rollout + gradient),
+    `render` (1M dam break, 3 frames at 1280x720).  Returns one line with its
+    CUDA-event time; not a benchmark value."""
+    import torch
+
+    from mtlphys_b200 import Engine, _abi, configs
+    from mtlphys_b200.batch import Batch
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    if which == "step":
+        w = configs.dam_break()
+        e = Engine(0)
+        e.set_params(w.params)
+        e.reset(w.n, w.scene, w.desc)
+        ms = timed(lambda: [e.step(w.dt, stream) for _ in range(3)])
+        e.check_errors()
+        return f"step: 3 steps of {w.n} particles in {ms:.3f} ms"
+    if which == "batch":
+        w = configs.batch_cubes()
+        b = Batch(0)
+        b.reset(w.counts, w.params, w.dts, w.scenes, w.descs)
+        ms = timed(lambda: [b.step(stream) for _ in range(3)])
+        b.check_errors()
+        return f"batch: 3 steps of {len(w.counts)} scenes ({w.n} particles) in {ms:.3f} ms"
+    if which == "adjoint":
+        w = configs.diff_cube(side=46, steps=20)
+        b = Batch(0)
+        b.reset([w.n], [w.params], [w.dt], [w.scene], [w.desc])
+        g = torch.zeros((w.n, 4), device="cuda")
+        g[:, 1] = 1.0 / w.n
+
+        def go():
+            b.rollout_forward(w.steps, 10, stream)
+            b.rollout_backward(g, None, stream)
+
+        ms = timed(go)
+        b.check_errors()
+        return f"adjoint: {w.steps}-step rollout + gradient of {w.n} particles in {ms:.3f} ms"
+    if which == "render":
+        w = configs.dam_break()
+        e = Engine(0)
+        e.set_params(w.params)
+        e.reset(w.n, w.scene, w.desc)
+        for _ in range(20):
+            e.step(w.dt, stream)
+        rp = _abi.default_render_params(width=1280, height=720)
+        rp.eye[:] = [14.0, 8.0, 15.0]
+        rp.target[:] = [4.3, 2.0, 4.3]
+        ms = timed(lambda: [e.render(rp, stream) for _ in range(3)])
+        return f"render: 3 frames of {w.n} particles at 1280x720 in {ms:.3f} ms"
+    raise SystemExit(f"unknown profile workload {which!r}: step, batch, adjoint or render")
 
 
 def main() -> None:
@@ -673,7 +794,12 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
+    ap.add_argument("--profile", choices=["step", "batch", "adjoint", "render"],
+                    help="run one fixed short workload for a profiler and exit (no bench line)")
     args = ap.parse_args()
+    if args.profile:
+        print(run_profile(args.profile), flush=True)
+        return
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
 

@@ -13,12 +13,11 @@ import subprocess
 
 import numpy as np
 
-from mtlphys_b200._abi import PBFParams, SceneDesc
+from .params import PBFParams, SceneDesc, as_desc, as_params
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmtlref.so")
-REFERENCE_ROOT = "/root/reference"
 
 _F = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -26,10 +25,12 @@ _U = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 
 
 def build(with_ref: bool | None = None) -> None:
-    """Compile the oracle (and the _ref cross-check when the reference
-    sources are present)."""
+    """Compile the oracle (and the _ref cross-check when $MTLPHYS_REFERENCE
+    names a reference checkout)."""
     target = ["all"] if with_ref is None else (["oracle", "ref"] if with_ref else ["oracle"])
-    subprocess.run(["make", "-s", "-C", HERE, *target], check=True)
+    ref_root = os.environ.get("MTLPHYS_REFERENCE", "")
+    extra = [f"REF={ref_root}"] if ref_root else []
+    subprocess.run(["make", "-s", "-C", HERE, *extra, *target], check=True)
 
 
 class Grid(C.Structure):
@@ -139,7 +140,7 @@ def _f4(a) -> np.ndarray:
 
 def grid(p: PBFParams) -> Grid:
     g = Grid()
-    rc = lib().or_make_grid(C.byref(p), C.byref(g))
+    rc = lib().or_make_grid(C.byref(as_params(p)), C.byref(g))
     if rc != 0:
         raise ValueError("invalid grid parameters")
     return g
@@ -184,7 +185,7 @@ def predict_f32(p: PBFParams, pos4, vel4, dt: float) -> np.ndarray:
 
 def seed_scene(p: PBFParams, scene: int, n: int, desc: SceneDesc | None = None) -> np.ndarray:
     out = np.empty((n, 4), np.float32)
-    rc = lib().or_seed_scene(C.byref(p), scene, C.byref(desc) if desc is not None else None, n, out)
+    rc = lib().or_seed_scene(C.byref(as_params(p)), scene, C.byref(as_desc(desc)) if desc is not None else None, n, out)
     if rc != 0:
         raise ValueError(f"or_seed_scene failed ({rc})")
     return out
@@ -209,7 +210,7 @@ def step(p: PBFParams, dt: float, pos4, vel4, sphere=None) -> dict:
     if sphere is not None:
         sph = np.ascontiguousarray(sphere, dtype=np.float64)
         assert sph.shape == (7,)
-    rc = lib().or_step(C.byref(p), C.c_float(dt), n, pos4, vel4, _ptr(sph), C.byref(so))
+    rc = lib().or_step(C.byref(as_params(p)), C.c_float(dt), n, pos4, vel4, _ptr(sph), C.byref(so))
     if rc != 0:
         raise ValueError(f"or_step failed ({rc})")
     if sphere is not None:
@@ -220,7 +221,7 @@ def step(p: PBFParams, dt: float, pos4, vel4, sphere=None) -> dict:
 def integrate_f32(p: PBFParams, dt: float, pos4, vel4):
     """Engine::integrate in FP32; returns new (pos4, vel4) arrays."""
     pos4, vel4 = _f4(pos4).copy(), _f4(vel4).copy()
-    lib().or_integrate_f32(C.byref(p), C.c_float(dt), len(pos4), pos4, vel4)
+    lib().or_integrate_f32(C.byref(as_params(p)), C.c_float(dt), len(pos4), pos4, vel4)
     return pos4, vel4
 
 
@@ -228,7 +229,7 @@ def mouse_pulse_f32(p: PBFParams, origin, direction, force, radius: float, pos4,
     """Engine::applyMousePulse in FP32; returns the new velocities."""
     vel4 = _f4(vel4).copy()
     v3 = lambda a: (C.c_float * 3)(*[float(x) for x in a])
-    lib().or_mouse_pulse_f32(C.byref(p), v3(origin), v3(direction), v3(force), C.c_float(radius),
+    lib().or_mouse_pulse_f32(C.byref(as_params(p)), v3(origin), v3(direction), v3(force), C.c_float(radius),
                              len(vel4), _f4(pos4), vel4)
     return vel4
 
@@ -238,7 +239,7 @@ def step_f64(p: PBFParams, dt: float, pos3, vel3, sphere=None) -> None:
     assert pos3.dtype == np.float64 and pos3.flags.c_contiguous
     assert vel3.dtype == np.float64 and vel3.flags.c_contiguous
     sph = None if sphere is None else sphere
-    rc = lib().or_step_f64(C.byref(p), C.c_double(dt), len(pos3), pos3, vel3, _ptr(sph))
+    rc = lib().or_step_f64(C.byref(as_params(p)), C.c_double(dt), len(pos3), pos3, vel3, _ptr(sph))
     if rc != 0:
         raise ValueError(f"or_step_f64 failed ({rc})")
 

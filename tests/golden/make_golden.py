@@ -3,7 +3,7 @@ compute shaders (engine/shaders/*.metal) compiled as host C++ by
 oracle/Makefile into oracle/_ref/libmtlref.so.
 
 Run in a checkout where the reference sources are present:
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=<reference checkout> && python tests/golden/make_golden.py
 The fixtures pin the FP64 oracle and the CUDA path to the reference's
 arithmetic.  Inputs follow the reference tests (tests/test_spatial.cpp,
 tests/test_pbf.cpp, tests/test_scan.cpp) and the reference engine's default
@@ -19,7 +19,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from mtlphys_b200 import _abi  # noqa: E402
+from oracle import params as _abi  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
