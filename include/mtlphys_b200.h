@@ -143,6 +143,28 @@ int mp_default_scene_desc(mp_scene_desc* out);
  * approximates as ~8072 before hard-coding 8000). */
 double mp_lattice_rest_density(double h, double spacing);
 
+/* ---- failure handling (no reference counterpart: the reference aborts the
+ *      process, engine/src/Engine.cpp:72-83, 407-413, 849-854, and creates its
+ *      buffers unchecked, :390-395) ------------------------------------------
+ * Device allocations.  Every device buffer of engines and batches is made by
+ * `alloc` and given back with `free_fn` (the one that made it, even after the
+ * allocator is replaced, and only once the device is idle).  alloc returns 0
+ * and a device pointer on `device`, or non-zero when it cannot: the call that
+ * needed the memory then returns MP_ERR_OUT_OF_MEMORY and leaves the engine or
+ * batch empty (no particles; steps do nothing) but usable: a later reset
+ * allocates again.  NULL restores cudaMalloc / cudaFree.  Process-wide;
+ * install it before the calls whose allocations it should see. */
+typedef int (*mp_device_alloc_fn)(void** ptr, size_t bytes, int device, void* user);
+typedef void (*mp_device_free_fn)(void* ptr, int device, void* user);
+int mp_set_device_allocator(mp_device_alloc_fn alloc, mp_device_free_fn free_fn, void* user);
+/* Bound, in polls, of every device-side wait of kernels enqueued after the
+ * call: the scan's decoupled look-back and the batch kernel's grid barrier
+ * (each poll naps 32-64 ns).  0 restores the defaults (2^22 and 2^24 polls).
+ * A wait that runs out sets MP_DEVERR_SPIN_LIMIT instead of hanging; see
+ * mp_exclusive_scan_status and mp_batch_check_errors.  Process-wide; engines
+ * and batches re-capture their CUDA graphs at their next step. */
+int mp_set_spin_limit(uint32_t polls);
+
 /* ---- engine lifetime: Engine.hpp:29-30, 41-44 ---------------------------- */
 /* Engine(MTL::Device*) — binds `device`, then reset(200'000) like
  * Engine.cpp:97-102. */
@@ -315,7 +337,16 @@ int mp_batch_get_sphere(mp_batch* b, uint32_t scene, float center[3], float velo
  * solver_iterations must stay the same (the hash grid does not change). */
 int mp_batch_set_params(mp_batch* b, uint32_t scene, const mp_pbf_params* params);
 int mp_batch_get_params(const mp_batch* b, uint32_t scene, mp_pbf_params* params);
+/* Wait for the batch's queued work and report its device error word (as
+ * mp_engine_check_errors).  When a grid barrier gave up (MP_ERR_SPIN_LIMIT),
+ * the launch left every block at its next barrier, so the state of that step
+ * is invalid, and every step after it did nothing; this call re-arms the
+ * batch, which steps again from its (invalid) state: restore or reset it. */
 int mp_batch_check_errors(mp_batch* b, uint32_t* bits);
+/* Test hook: every grid barrier of the following steps waits for `extra`
+ * more blocks than the launch has (0 = normal), so every wait runs out after
+ * the mp_set_spin_limit bound.  For failure-path tests only. */
+int mp_batch_debug_barrier_extra(mp_batch* b, uint32_t extra);
 
 /* ---- differentiable rollouts (no reference counterpart: the reference
  *      engine is not differentiable) ------------------------------------------
@@ -375,6 +406,19 @@ int mp_batch_restore(mp_batch* b, const void* host, size_t bytes);
 size_t mp_exclusive_scan_scratch_bytes(uint32_t n);
 int mp_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n,
                       void* scratch, size_t scratch_bytes, mp_stream stream);
+/* Waits for `stream` and reports whether the last scan that used `scratch`
+ * (NULL: the static scratch of mp_exclusive_scan_noalloc) completed:
+ * MP_ERR_SPIN_LIMIT when its look-back wait gave up (that scan's output is
+ * wrong), MP_OK otherwise; the error word is cleared.  The scans themselves
+ * are asynchronous and return MP_OK once enqueued. */
+int mp_exclusive_scan_status(const void* scratch, mp_stream stream);
+/* Test hook: mp_exclusive_scan with the tile ticket starting at
+ * `first_ticket`.  A ticket that is not a multiple of the tile count splits
+ * the tiles across two epochs, so the look-back of the first tile launched
+ * waits for descriptors no tile writes and gives up after the
+ * mp_set_spin_limit bound.  For failure-path tests only. */
+int mp_debug_exclusive_scan_from_ticket(const uint32_t* in, uint32_t* out, uint32_t n, void* scratch,
+                                        size_t scratch_bytes, uint64_t first_ticket, mp_stream stream);
 
 /* The same exclusive scan without any device allocation, for callers that
  * cannot allocate when they need it (a frame loop with a fixed per-frame
@@ -385,6 +429,9 @@ int mp_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n,
  * MP_ERR_INVALID_ARGUMENT.  `in` and `out` are device pointers on the current
  * device.  The first call on each device looks up the array's address (set-up
  * with that device current); make that first call before any stream capture.
+ * Calls outside stream capture look the address up again, so it follows a
+ * device reset.  A look-back that gives up is reported by
+ * mp_exclusive_scan_status(NULL, stream).
  * All calls share the one array, so calls that overlap on the GPU (other
  * streams, other host threads) race: order them on one stream. */
 int mp_exclusive_scan_noalloc(const uint32_t* in, uint32_t* out, uint32_t n, mp_stream stream);

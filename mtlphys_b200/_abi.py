@@ -233,7 +233,16 @@ PROTOTYPES = {
     "mp_exclusive_scan_scratch_bytes": (_SZ, [_U32]),
     "mp_exclusive_scan": (_INT, [_VP, _VP, _U32, _VP, _SZ, _VP]),
     "mp_exclusive_scan_noalloc": (_INT, [_VP, _VP, _U32, _VP]),
+    "mp_exclusive_scan_status": (_INT, [_VP, _VP]),
+    "mp_debug_exclusive_scan_from_ticket": (_INT, [_VP, _VP, _U32, _VP, _SZ, C.c_uint64, _VP]),
+    "mp_set_spin_limit": (_INT, [_U32]),
+    "mp_set_device_allocator": (_INT, [_VP, _VP, _VP]),
+    "mp_batch_debug_barrier_extra": (_INT, [_VP, _U32]),
 }
+
+# mp_device_alloc_fn / mp_device_free_fn
+DEVICE_ALLOC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_void_p), C.c_size_t, C.c_int, C.c_void_p)
+DEVICE_FREE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_void_p)
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmtlphys_b200.so")
 

@@ -62,6 +62,8 @@ struct mp_batch {
     cudaStream_t cap_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    uint32_t graph_spin_epoch = 0;  // spin limits the captured graph was made with
+    uint32_t bar_extra = 0;         // test hook: mp_batch_debug_barrier_extra
 
     // ---- differentiable rollouts ----
     // One recorded step: the record arrays of the step kernel plus its own
@@ -90,14 +92,14 @@ struct mp_batch {
 
     int ensure_tape(uint32_t nslots) {
         if (slots.size() >= nslots) return MP_OK;
-        if (tape_block) cudaFree(tape_block);
+        dev_free(tape_block);
         tape_block = nullptr;
         slots.clear();
         const size_t cap = cap_slots(), K = iterations, v4 = cap * 16, u = cap * 4;
         const size_t per = al(sizeof(SceneDev) * std::max<uint32_t>(S, 1u)) +
                            al(sizeof(SphereState) * std::max<uint32_t>(S, 1u)) + al(v4) + 2 * al(u) +
                            al((size_t(max_cells) + 1) * 4) + K * (2 * al(v4) + al(9 * u) + al(u));
-        MP_CUDA(cudaMalloc(&tape_block, per * nslots));
+        MP_ALLOC(tape_block, per * nslots, device);
         char* p = static_cast<char*>(tape_block);
         auto take = [&](size_t bytes) {
             char* r = p;
@@ -125,12 +127,12 @@ struct mp_batch {
 
     int ensure_ckpts(uint32_t n) {
         if (ckpts.size() >= n) return MP_OK;
-        if (ckpt_block) cudaFree(ckpt_block);
+        dev_free(ckpt_block);
         ckpt_block = nullptr;
         ckpts.clear();
         const size_t v4 = cap_slots() * 16, sc = al(sizeof(SceneDev) * std::max<uint32_t>(S, 1u));
         const size_t per = 2 * al(v4) + sc;
-        MP_CUDA(cudaMalloc(&ckpt_block, per * n));
+        MP_ALLOC(ckpt_block, per * n, device);
         char* p = static_cast<char*>(ckpt_block);
         for (uint32_t i = 0; i < n; ++i) {
             Saved sv{reinterpret_cast<float4*>(p), reinterpret_cast<float4*>(p + al(v4)),
@@ -146,7 +148,7 @@ struct mp_batch {
         const size_t cap = cap_slots(), v4 = al(cap * 16), u = al(cap * 4);
         const size_t gbytes = al(sizeof(double) * kGradStride * std::max<uint32_t>(S, 1u));
         const size_t total = 8 * v4 + 5 * u + gbytes;
-        MP_CUDA(cudaMalloc(&adj_block, total));
+        MP_ALLOC(adj_block, total, device);
         MP_CUDA(cudaMemset(adj_block, 0, total));
         char* p = static_cast<char*>(adj_block);
         auto v = [&]() { float4* r = reinterpret_cast<float4*>(p); p += v4; return r; };
@@ -176,8 +178,7 @@ struct mp_batch {
     }
 
     void free_rollout() {
-        for (void* p : {tape_block, ckpt_block, adj_block})
-            if (p) cudaFree(p);
+        for (void* p : {tape_block, ckpt_block, adj_block}) dev_free(p);
         tape_block = ckpt_block = adj_block = nullptr;
         slots.clear();
         ckpts.clear();
@@ -203,7 +204,7 @@ struct mp_batch {
     // One step of every scene in one launch, kept in tape slot `i`.
     int enqueue_recorded(uint32_t i, cudaStream_t s) {
         const Slot& sl = slots[i];
-        BatchArgs args = a;
+        BatchArgs args = launch_args();
         args.scene_begin = 0;
         args.scene_end = S;
         args.p_begin = 0;
@@ -237,8 +238,7 @@ struct mp_batch {
     }
     void free_all() {
         drop_graph();
-        for (void* p : {particle_block, cell_block, small_block, static_cast<void*>(scenes)})
-            if (p) cudaFree(p);
+        for (void* p : {particle_block, cell_block, small_block, static_cast<void*>(scenes)}) dev_free(p);
         particle_block = cell_block = small_block = nullptr;
         scenes = nullptr;
         a = BatchArgs{};
@@ -258,11 +258,19 @@ struct mp_batch {
         return uint32_t(std::max(1, per_sm) * std::max(1, sms));
     }
 
+    // launch arguments with the current bound of the barrier wait
+    BatchArgs launch_args() const {
+        BatchArgs args = a;
+        args.spin_limit = barrier_spin_limit();
+        args.bar_extra = bar_extra;
+        return args;
+    }
+
     int enqueue(cudaStream_t s) {
         if (N == 0) return MP_OK;
         const uint32_t nb = blocks();
         if (!serial) {
-            BatchArgs args = a;
+            BatchArgs args = launch_args();
             args.scene_begin = 0;
             args.scene_end = S;
             args.p_begin = 0;
@@ -277,7 +285,7 @@ struct mp_batch {
         for (uint32_t sc = 0; sc < S; ++sc) {
             if (counts[sc] == 0) continue;
             const uint32_t need = uint32_t((uint64_t(counts[sc]) + block - 1) / block);
-            BatchArgs args = a;
+            BatchArgs args = launch_args();
             args.scene_begin = sc;
             args.scene_end = sc + 1;
             args.p_begin = p0[sc];
@@ -291,6 +299,7 @@ struct mp_batch {
     // One step of every scene (graph replay in graph mode).
     int step(cudaStream_t s) {
         if (!graph_mode) return enqueue(s);
+        if (gexec && graph_spin_epoch != spin_limit_epoch()) drop_graph();
         if (!gexec) {
             if (!cap_stream) MP_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
             MP_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
@@ -304,6 +313,7 @@ struct mp_batch {
             if (ce != cudaSuccess) return fail(MP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
             graph = g;
             MP_CUDA(cudaGraphInstantiate(&gexec, graph, 0));
+            graph_spin_epoch = spin_limit_epoch();
         }
         MP_CUDA(cudaGraphLaunch(gexec, s));
         return MP_OK;
@@ -434,65 +444,83 @@ int mp_batch_reset(mp_batch* b, uint32_t nscenes, const uint32_t* counts, const 
     for (uint32_t s = 0; s < nscenes; ++s) b->p0[s] = hs[s].p0;
     b->host_scenes = hs;
     b->max_cells = uint32_t(worst_cells);
-    // particles
-    const uint32_t cap = round_up(std::max<uint32_t>(b->N, 1u), 256u);
-    const size_t v4 = size_t(cap) * 16, u = size_t(cap) * 4;
-    const size_t longs = (size_t(cap) / kSegMax + 2) * 4;
-    const size_t ptotal = 5 * v4 + 19 * u + longs + 32 * 256;
-    MP_CUDA(cudaMalloc(&b->particle_block, ptotal));
-    MP_CUDA(cudaMemset(b->particle_block, 0, ptotal));
-    char* pb = static_cast<char*>(b->particle_block);
-    auto take = [&](size_t bytes) {
-        char* r = pb;
-        pb += (bytes + 255) & ~size_t(255);
-        return r;
-    };
-    BatchArgs& a = b->a;
-    a.pos = reinterpret_cast<float4*>(take(v4));
-    a.vel = reinterpret_cast<float4*>(take(v4));
-    a.prev = reinterpret_cast<float4*>(take(v4));
-    a.sorted_a = reinterpret_cast<float4*>(take(v4));
-    a.sorted_b = reinterpret_cast<float4*>(take(v4));
-    a.hash = reinterpret_cast<uint32_t*>(take(u));
-    a.off = reinterpret_cast<uint32_t*>(take(u));
-    a.tmp = reinterpret_cast<uint32_t*>(take(u));
-    a.sidx = reinterpret_cast<uint32_t*>(take(u));
-    a.scell = reinterpret_cast<uint32_t*>(take(u));
-    a.ncount = reinterpret_cast<uint32_t*>(take(u));
-    a.lambdas = reinterpret_cast<float*>(take(u));
-    a.foam = reinterpret_cast<float*>(take(u));
-    uint32_t* so = reinterpret_cast<uint32_t*>(take(u));
-    a.scene_of = so;
-    a.row_masks = reinterpret_cast<uint32_t*>(take(9 * u));
-    a.mask_overflow = reinterpret_cast<uint32_t*>(take(u));
-    a.mask_stride = cap;
-    a.long_list = reinterpret_cast<uint32_t*>(take(longs));
-    // cells: counts + cstart for the worst case (every scene's whole box)
-    const size_t clen = size_t(b->max_cells) + 1;
-    const size_t tiles = clen / 128 + 2;
-    const size_t cbytes = ((clen * 4 + 255) & ~size_t(255));
-    MP_CUDA(cudaMalloc(&b->cell_block, 2 * cbytes + tiles * 4));
-    MP_CUDA(cudaMemset(b->cell_block, 0, 2 * cbytes + tiles * 4));
-    a.counts = static_cast<uint32_t*>(b->cell_block);
-    a.cstart = reinterpret_cast<uint32_t*>(static_cast<char*>(b->cell_block) + cbytes);
-    a.tile_sums = reinterpret_cast<uint32_t*>(static_cast<char*>(b->cell_block) + 2 * cbytes);
-    a.max_cells = b->max_cells;
-    MP_CUDA(cudaMalloc(&b->small_block, 256));
-    MP_CUDA(cudaMemset(b->small_block, 0, 256));
-    uint32_t* sm = static_cast<uint32_t*>(b->small_block);
-    a.long_count = sm + 0;
-    a.total_cells = sm + 1;
-    a.err = sm + 2;
-    a.bar_count = reinterpret_cast<unsigned*>(sm + 32);
-    a.bar_gen = reinterpret_cast<unsigned*>(sm + 33);
-    MP_CUDA(cudaMalloc(&b->scenes, sizeof(SceneDev) * std::max<uint32_t>(nscenes, 1u)));
-    a.scenes = b->scenes;
-    a.iterations = iters;
-    int rc = b->upload_scenes();
-    if (rc != MP_OK) return rc;
-    if (total) {
-        MP_CUDA(cudaMemcpy(a.pos, pos.data(), 16 * size_t(total), cudaMemcpyHostToDevice));
-        MP_CUDA(cudaMemcpy(so, scene_of.data(), 4 * size_t(total), cudaMemcpyHostToDevice));
+    // A failed allocation leaves the batch empty (no scenes), not half-built.
+    const int arc = [&]() -> int {
+        // particles
+        const uint32_t cap = round_up(std::max<uint32_t>(b->N, 1u), 256u);
+        const size_t v4 = size_t(cap) * 16, u = size_t(cap) * 4;
+        const size_t longs = (size_t(cap) / kSegMax + 2) * 4;
+        const size_t ptotal = 5 * v4 + 19 * u + longs + 32 * 256;
+        MP_ALLOC(b->particle_block, ptotal, b->device);
+        MP_CUDA(cudaMemset(b->particle_block, 0, ptotal));
+        char* pb = static_cast<char*>(b->particle_block);
+        auto take = [&](size_t bytes) {
+            char* r = pb;
+            pb += (bytes + 255) & ~size_t(255);
+            return r;
+        };
+        BatchArgs& a = b->a;
+        a.pos = reinterpret_cast<float4*>(take(v4));
+        a.vel = reinterpret_cast<float4*>(take(v4));
+        a.prev = reinterpret_cast<float4*>(take(v4));
+        a.sorted_a = reinterpret_cast<float4*>(take(v4));
+        a.sorted_b = reinterpret_cast<float4*>(take(v4));
+        a.hash = reinterpret_cast<uint32_t*>(take(u));
+        a.off = reinterpret_cast<uint32_t*>(take(u));
+        a.tmp = reinterpret_cast<uint32_t*>(take(u));
+        a.sidx = reinterpret_cast<uint32_t*>(take(u));
+        a.scell = reinterpret_cast<uint32_t*>(take(u));
+        a.ncount = reinterpret_cast<uint32_t*>(take(u));
+        a.lambdas = reinterpret_cast<float*>(take(u));
+        a.foam = reinterpret_cast<float*>(take(u));
+        uint32_t* so = reinterpret_cast<uint32_t*>(take(u));
+        a.scene_of = so;
+        a.row_masks = reinterpret_cast<uint32_t*>(take(9 * u));
+        a.mask_overflow = reinterpret_cast<uint32_t*>(take(u));
+        a.mask_stride = cap;
+        a.long_list = reinterpret_cast<uint32_t*>(take(longs));
+        // cells: counts + cstart for the worst case (every scene's whole box)
+        const size_t clen = size_t(b->max_cells) + 1;
+        const size_t tiles = clen / 128 + 2;
+        const size_t cbytes = ((clen * 4 + 255) & ~size_t(255));
+        MP_ALLOC(b->cell_block, 2 * cbytes + tiles * 4, b->device);
+        MP_CUDA(cudaMemset(b->cell_block, 0, 2 * cbytes + tiles * 4));
+        a.counts = static_cast<uint32_t*>(b->cell_block);
+        a.cstart = reinterpret_cast<uint32_t*>(static_cast<char*>(b->cell_block) + cbytes);
+        a.tile_sums = reinterpret_cast<uint32_t*>(static_cast<char*>(b->cell_block) + 2 * cbytes);
+        a.max_cells = b->max_cells;
+        MP_ALLOC(b->small_block, 256, b->device);
+        MP_CUDA(cudaMemset(b->small_block, 0, 256));
+        uint32_t* sm = static_cast<uint32_t*>(b->small_block);
+        a.long_count = sm + 0;
+        a.total_cells = sm + 1;
+        a.err = sm + 2;
+        a.bar_count = reinterpret_cast<unsigned*>(sm + 32);
+        a.bar_gen = reinterpret_cast<unsigned*>(sm + 33);
+        a.abort = sm + 48;
+        MP_ALLOC(b->scenes, sizeof(SceneDev) * std::max<uint32_t>(nscenes, 1u), b->device);
+        a.scenes = b->scenes;
+        a.iterations = iters;
+        int rc = b->upload_scenes();
+        if (rc != MP_OK) return rc;
+        if (total) {
+            MP_CUDA(cudaMemcpy(a.pos, pos.data(), 16 * size_t(total), cudaMemcpyHostToDevice));
+            MP_CUDA(cudaMemcpy(so, scene_of.data(), 4 * size_t(total), cudaMemcpyHostToDevice));
+        }
+        return MP_OK;
+    }();
+    if (arc != MP_OK) {
+        b->free_all();
+        b->S = b->N = 0;
+        b->counts.clear();
+        b->p0.clear();
+        b->scene_ids.clear();
+        b->params.clear();
+        b->descs.clear();
+        b->dts.clear();
+        b->host_scenes.clear();
+        b->max_cells = 0;
+        return arc;
     }
     // launch shape: the cached autotuning result for this size, if any
     {
@@ -580,7 +608,7 @@ int mp_batch_autotune(mp_batch* b, uint32_t steps, mp_batch_tuning* best) {
     // restored afterwards: tuning does not advance the simulation.
     const size_t v4 = size_t(b->N) * 16;
     void* save = nullptr;
-    MP_CUDA(cudaMalloc(&save, 2 * v4 + sizeof(SceneDev) * b->S));
+    MP_ALLOC(save, 2 * v4 + sizeof(SceneDev) * b->S, b->device);
     auto snapshot = [&](bool restore) -> int {
         char* sv = static_cast<char*>(save);
         const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
@@ -630,7 +658,7 @@ int mp_batch_autotune(mp_batch* b, uint32_t steps, mp_batch_tuning* best) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     const int rc2 = snapshot(true);
-    cudaFree(save);
+    dev_free(save);
     b->graph_mode = saved_graph;
     if (rc != MP_OK || rc2 != MP_OK) {
         b->block = saved_block;
@@ -919,10 +947,24 @@ int mp_batch_check_errors(mp_batch* b, uint32_t* bits) {
     if (b->a.err) {
         MP_CUDA(cudaMemcpy(&w, b->a.err, 4, cudaMemcpyDeviceToHost));
         MP_CUDA(cudaMemset(b->a.err, 0, 4));
+        if (w & kDevErrSpin) {
+            // a barrier wait gave up: the launch left the barrier counter
+            // mid-count and the abort flag set; re-arm both
+            MP_CUDA(cudaMemset(b->a.bar_count, 0, sizeof(unsigned)));
+            MP_CUDA(cudaMemset(b->a.abort, 0, sizeof(uint32_t)));
+        }
     }
     if (bits) *bits = w;
     if (w & kDevErrSpin) return fail(MP_ERR_SPIN_LIMIT, "a bounded device wait gave up (bits 0x%x)", w);
     if (w) return fail(MP_ERR_DEVICE, "device error word 0x%x", w);
+    return MP_OK;
+}
+
+int mp_batch_debug_barrier_extra(mp_batch* b, uint32_t extra) {
+    if (!b) return fail(MP_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (extra > 1024) return fail(MP_ERR_INVALID_ARGUMENT, "extra = %u > 1024", extra);
+    b->bar_extra = extra;
+    b->drop_graph();
     return MP_OK;
 }
 

@@ -15,9 +15,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <map>
+#include <mutex>
 #include <random>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "host_common.h"
@@ -55,6 +58,76 @@ int fail(int code, const char* fmt, ...) {
 void record_error(const char* msg) { g_err = msg; }
 
 const char* last_error() { return g_err.c_str(); }
+
+// ---- bounds of the device-side waits (mp_set_spin_limit) --------------------
+namespace {
+std::atomic<uint32_t> g_scan_spins{kDefaultScanSpinLimit};
+std::atomic<uint32_t> g_barrier_spins{kDefaultBarrierSpinLimit};
+std::atomic<uint32_t> g_spin_epoch{0};
+}  // namespace
+
+uint32_t scan_spin_limit() { return g_scan_spins.load(); }
+uint32_t barrier_spin_limit() { return g_barrier_spins.load(); }
+uint32_t spin_limit_epoch() { return g_spin_epoch.load(); }
+
+// ---- device allocations (mp_set_device_allocator) ---------------------------
+namespace {
+struct Allocator {
+    mp_device_alloc_fn alloc = nullptr;  // nullptr: cudaMalloc / cudaFree
+    mp_device_free_fn free = nullptr;
+    void* user = nullptr;
+};
+std::mutex g_alloc_lock;
+Allocator g_alloc;
+// who made each live block (it is given back to the same allocator)
+std::unordered_map<void*, std::pair<Allocator, int>> g_blocks;
+}  // namespace
+
+int dev_alloc(void** p, size_t bytes, int device) {
+    *p = nullptr;
+    Allocator a;
+    {
+        std::lock_guard<std::mutex> lock(g_alloc_lock);
+        a = g_alloc;
+    }
+    void* ptr = nullptr;
+    if (a.alloc) {
+        if (a.alloc(&ptr, bytes, device, a.user) != 0 || !ptr)
+            return fail(MP_ERR_OUT_OF_MEMORY, "device allocator refused %zu bytes on device %d", bytes,
+                        device);
+    } else {
+        const cudaError_t e = cudaMalloc(&ptr, bytes);
+        if (e != cudaSuccess)
+            return fail(e == cudaErrorMemoryAllocation ? MP_ERR_OUT_OF_MEMORY : MP_ERR_CUDA,
+                        "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    std::lock_guard<std::mutex> lock(g_alloc_lock);
+    g_blocks[ptr] = {a, device};
+    *p = ptr;
+    return MP_OK;
+}
+
+void dev_free(void* p) {
+    if (!p) return;
+    std::pair<Allocator, int> owner;
+    {
+        std::lock_guard<std::mutex> lock(g_alloc_lock);
+        auto it = g_blocks.find(p);
+        if (it == g_blocks.end()) return;
+        owner = it->second;
+        g_blocks.erase(it);
+    }
+    if (owner.first.alloc) {
+        // a caller's allocator may hand the block out again at once: give it
+        // back only when no queued kernel can still use it (cudaFree waits
+        // by itself)
+        DeviceGuard g(owner.second);
+        cudaDeviceSynchronize();
+        if (owner.first.free) owner.first.free(p, owner.second, owner.first.user);
+    } else {
+        cudaFree(p);
+    }
+}
 
 // Grid of buildSpatialBuffers (Engine.cpp:398-403, 443-451).
 int make_grid(const mp_pbf_params& p, GridDev& g) {
@@ -379,6 +452,7 @@ struct mp_engine {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     float graph_dt = 0.0f;
+    uint32_t graph_spin_epoch = 0;  // spin limits the captured graph was made with
     // profiling
     EventTimer* timer = nullptr;
     // render targets (Engine::ensureRenderTargets, Engine.cpp:351-377)
@@ -388,10 +462,10 @@ struct mp_engine {
 
     int ensure_render_targets(uint32_t w, uint32_t h) {
         if (render_block && w == render_w && h == render_h) return MP_OK;
-        if (render_block) cudaFree(render_block);
+        dev_free(render_block);
         render_block = nullptr;
         const size_t px = size_t(w) * h, plane = (px * 4 + 255) & ~size_t(255);
-        MP_CUDA(cudaMalloc(&render_block, 4 * plane + 4 * plane));
+        MP_ALLOC(render_block, 4 * plane + 4 * plane, device);
         char* p = static_cast<char*>(render_block);
         rb.depth = reinterpret_cast<uint32_t*>(p);
         rb.thick = reinterpret_cast<float*>(p + plane);
@@ -410,18 +484,23 @@ struct mp_engine {
         graph = nullptr;
     }
     void free_particles() {
-        if (particle_block) cudaFree(particle_block);
-        if (list_block) cudaFree(list_block);
+        dev_free(particle_block);
+        dev_free(list_block);
         particle_block = nullptr;
         list_block = nullptr;
+        d.pos = d.vel = d.prev = d.sorted_a = d.sorted_b = nullptr;
+        d.hash = d.off = d.tmp = d.sidx = d.scell = d.ncount = d.long_list = nullptr;
+        d.lambdas = d.foam = nullptr;
         d.row_masks = nullptr;
         d.mask_overflow = nullptr;
         d.mask_stride = 0;
         n_alloc = 0;
     }
     void free_cells() {
-        if (cell_block) cudaFree(cell_block);
+        dev_free(cell_block);
         cell_block = nullptr;
+        d.counts = d.cstart = nullptr;
+        d.scan_ticket = d.scan_status = nullptr;
         cells_alloc = 0;
     }
     ~mp_engine() {
@@ -431,8 +510,8 @@ struct mp_engine {
         if (cap_stream) cudaStreamDestroy(cap_stream);
         free_particles();
         free_cells();
-        if (small_block) cudaFree(small_block);
-        if (render_block) cudaFree(render_block);
+        dev_free(small_block);
+        dev_free(render_block);
     }
 
     int alloc_particles(uint32_t count) {
@@ -442,7 +521,7 @@ struct mp_engine {
         const size_t v4 = size_t(cap) * 16, u = size_t(cap) * 4;
         const size_t longs = (size_t(cap) / mpb::kSegMax + 2) * 4;
         const size_t total = 5 * v4 + 8 * u + longs + 16 * 256;
-        MP_CUDA(cudaMalloc(&particle_block, total));
+        MP_ALLOC(particle_block, total, device);
         char* b = static_cast<char*>(particle_block);
         auto take = [&](size_t bytes) {
             char* r = b;
@@ -465,7 +544,7 @@ struct mp_engine {
         d.long_list = reinterpret_cast<uint32_t*>(take(longs));
         MP_CUDA(cudaMemset(particle_block, 0, total));
         // 9 row masks (4 bytes each) + an overflow flag per particle
-        MP_CUDA(cudaMalloc(&list_block, 10 * u));
+        MP_ALLOC(list_block, 10 * u, device);
         d.row_masks = static_cast<uint32_t*>(list_block);
         d.mask_overflow = d.row_masks + 9 * size_t(cap);
         d.mask_stride = cap;
@@ -480,7 +559,7 @@ struct mp_engine {
         const uint32_t tiles = mpb::scan_tiles_for(len);
         const size_t cb = ((len * 4 + 255) & ~size_t(255));
         const size_t total = 2 * cb + size_t(tiles) * 8 + 256;
-        MP_CUDA(cudaMalloc(&cell_block, total));
+        MP_ALLOC(cell_block, total, device);
         MP_CUDA(cudaMemset(cell_block, 0, total));
         char* b = static_cast<char*>(cell_block);
         d.counts = reinterpret_cast<uint32_t*>(b);
@@ -494,13 +573,24 @@ struct mp_engine {
 
     int alloc_small() {
         if (small_block) return MP_OK;
-        MP_CUDA(cudaMalloc(&small_block, 256));
+        MP_ALLOC(small_block, 256, device);
         MP_CUDA(cudaMemset(small_block, 0, 256));
         char* b = static_cast<char*>(small_block);
         d.long_count = reinterpret_cast<uint32_t*>(b);
         d.err = reinterpret_cast<uint32_t*>(b + 4);
         d.sphere = reinterpret_cast<mpb::SphereState*>(b + 64);
         return MP_OK;
+    }
+
+    // false after an allocation failed: the engine holds no particles and
+    // launches nothing until a reset or set_params allocates again
+    bool ready() const { return particle_block && cell_block && small_block; }
+
+    // a failed allocation leaves the engine empty, not half-built
+    int emptied(int rc) {
+        drop_graph();
+        n = 0;
+        return rc;
     }
 
     StepConsts consts(float dt) const {
@@ -597,7 +687,7 @@ int mp_engine_set_params(mp_engine* e, const mp_pbf_params* p) {
     rc = make_grid(*p, grid);
     if (rc != MP_OK) return rc;
     rc = e->alloc_cells(grid.cells);
-    if (rc != MP_OK) return rc;
+    if (rc != MP_OK) return e->emptied(rc);
     e->params = *p;
     e->grid = grid;
     e->drop_graph();
@@ -633,9 +723,10 @@ int mp_engine_reset_scene(mp_engine* e, uint32_t n, uint32_t scene, const mp_sce
     if (rc != MP_OK) return rc;
     DeviceGuard g(e->device);
     rc = make_grid(e->params, e->grid);
-    if (rc == MP_OK) rc = e->alloc_cells(e->grid.cells);
-    if (rc == MP_OK) rc = e->alloc_particles(n);
     if (rc != MP_OK) return rc;
+    rc = e->alloc_cells(e->grid.cells);
+    if (rc == MP_OK) rc = e->alloc_particles(n);
+    if (rc != MP_OK) return e->emptied(rc);
     e->drop_graph();
     e->scene = scene;
     e->desc = dd;
@@ -664,6 +755,7 @@ int mp_engine_reset_scene(mp_engine* e, uint32_t n, uint32_t scene, const mp_sce
 int mp_engine_step(mp_engine* e, float dt, mp_stream stream) {
     if (!e) return fail(MP_ERR_INVALID_ARGUMENT, "NULL engine");
     if (!(dt > 0.0f)) return MP_OK;  // Engine.cpp:686
+    if (!e->ready()) return MP_OK;   // emptied by a failed allocation
     DeviceGuard g(e->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (e->timer) {
@@ -674,7 +766,7 @@ int mp_engine_step(mp_engine* e, float dt, mp_stream stream) {
         return e->enqueue_step(dt, s, e->timer);
     }
     if (!e->graph_mode) return e->enqueue_step(dt, s);
-    if (!e->gexec || e->graph_dt != dt) {
+    if (!e->gexec || e->graph_dt != dt || e->graph_spin_epoch != mpb::spin_limit_epoch()) {
         e->drop_graph();
         if (!e->cap_stream) MP_CUDA(cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking));
         MP_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
@@ -689,6 +781,7 @@ int mp_engine_step(mp_engine* e, float dt, mp_stream stream) {
         e->graph = graph;
         MP_CUDA(cudaGraphInstantiate(&e->gexec, e->graph, 0));
         e->graph_dt = dt;
+        e->graph_spin_epoch = mpb::spin_limit_epoch();
     }
     MP_CUDA(cudaGraphLaunch(e->gexec, s));
     return MP_OK;
@@ -696,6 +789,7 @@ int mp_engine_step(mp_engine* e, float dt, mp_stream stream) {
 
 int mp_engine_build_spatial_hash(mp_engine* e, mp_stream stream) {
     if (!e) return fail(MP_ERR_INVALID_ARGUMENT, "NULL engine");
+    if (!e->ready()) return MP_OK;
     DeviceGuard g(e->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const StepConsts c = e->consts(1.0f);
@@ -846,7 +940,7 @@ int mp_engine_get_sphere(mp_engine* e, float center[3], float velocity[3], float
 
 int mp_engine_integrate(mp_engine* e, float dt, mp_stream stream) {
     if (!e) return fail(MP_ERR_INVALID_ARGUMENT, "NULL engine");
-    if (!(dt > 0.0f)) return MP_OK;
+    if (!(dt > 0.0f) || !e->ready()) return MP_OK;
     DeviceGuard g(e->device);
     const mp_pbf_params& p = e->params;
     mpb::IntegrateConsts c{};
@@ -871,6 +965,7 @@ int mp_engine_integrate(mp_engine* e, float dt, mp_stream stream) {
 int mp_engine_apply_mouse_pulse(mp_engine* e, const float ray_origin[3], const float ray_dir[3],
                                 const float force[3], float radius, mp_stream stream) {
     if (!e || !ray_origin || !ray_dir || !force) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!e->ready()) return MP_OK;
     DeviceGuard g(e->device);
     mpb::MouseConsts c{};
     c.n = e->n;
@@ -892,6 +987,8 @@ int mp_engine_apply_mouse_pulse(mp_engine* e, const float ray_origin[3], const f
 
 int mp_engine_render(mp_engine* e, const mp_render_params* rp, float* rgba, mp_stream stream) {
     if (!e || !rp) return fail(MP_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!e->ready())
+        return fail(MP_ERR_INVALID_ARGUMENT, "the engine holds no particles since an allocation failed");
     mpb::RenderConsts c;
     int rc = mpb::make_render_consts(*rp, e->params, e->n, e->scene == MP_SCENE_SPHERE_DROP, c);
     if (rc != MP_OK) return rc;
@@ -1000,6 +1097,22 @@ int mp_engine_synchronize(mp_engine* e) {
     return MP_OK;
 }
 
+int mp_set_spin_limit(uint32_t polls) {
+    g_scan_spins.store(polls ? polls : kDefaultScanSpinLimit);
+    g_barrier_spins.store(polls ? polls : kDefaultBarrierSpinLimit);
+    g_spin_epoch.fetch_add(1);
+    return MP_OK;
+}
+
+int mp_set_device_allocator(mp_device_alloc_fn alloc, mp_device_free_fn free_fn, void* user) {
+    if (alloc && !free_fn) return fail(MP_ERR_INVALID_ARGUMENT, "an allocator needs a free function");
+    std::lock_guard<std::mutex> lock(g_alloc_lock);
+    g_alloc.alloc = alloc;
+    g_alloc.free = alloc ? free_fn : nullptr;
+    g_alloc.user = alloc ? user : nullptr;
+    return MP_OK;
+}
+
 size_t mp_exclusive_scan_scratch_bytes(uint32_t n) {
     return 256 + size_t(mpb::scan_tiles_for(n)) * 8;
 }
@@ -1023,6 +1136,51 @@ int mp_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, void* scrat
                                            reinterpret_cast<uint32_t*>(b + 8), s);
     if (e != cudaSuccess) return fail(MP_ERR_CUDA, "scan launch: %s", cudaGetErrorString(e));
     return MP_OK;
+}
+
+int mp_debug_exclusive_scan_from_ticket(const uint32_t* in, uint32_t* out, uint32_t n, void* scratch,
+                                        size_t scratch_bytes, uint64_t first_ticket, mp_stream stream) {
+    if (n == 0) return MP_OK;
+    if (!in || !out || !scratch) return fail(MP_ERR_INVALID_ARGUMENT, "NULL pointer");
+    const size_t need = mp_exclusive_scan_scratch_bytes(n);
+    if (scratch_bytes < need)
+        return fail(MP_ERR_INVALID_ARGUMENT, "scratch of %zu bytes, need %zu", scratch_bytes, need);
+    if (reinterpret_cast<uintptr_t>(scratch) & 7u)
+        return fail(MP_ERR_INVALID_ARGUMENT, "scratch must be 8-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    MP_CUDA(cudaMemsetAsync(scratch, 0, need, s));
+    // pageable source: the call returns once the value is staged
+    const unsigned long long ticket = first_ticket;
+    MP_CUDA(cudaMemcpyAsync(scratch, &ticket, sizeof(ticket), cudaMemcpyHostToDevice, s));
+    char* b = static_cast<char*>(scratch);
+    const cudaError_t e = mpb::launch_scan(in, out, n, reinterpret_cast<unsigned long long*>(b + 256),
+                                           reinterpret_cast<unsigned long long*>(b),
+                                           mpb::scan_tiles_for(n), false,
+                                           reinterpret_cast<uint32_t*>(b + 8), s);
+    if (e != cudaSuccess) return fail(MP_ERR_CUDA, "scan launch: %s", cudaGetErrorString(e));
+    return MP_OK;
+}
+
+int mp_exclusive_scan_status(const void* scratch, mp_stream stream) {
+    uint32_t* word = nullptr;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (scratch) {
+        if (reinterpret_cast<uintptr_t>(scratch) & 7u)
+            return fail(MP_ERR_INVALID_ARGUMENT, "scratch must be 8-byte aligned");
+        word = reinterpret_cast<uint32_t*>(static_cast<char*>(const_cast<void*>(scratch)) + 8);
+    } else {
+        const int rc = mpb::noalloc_scan_error_word(s, &word);
+        if (rc != MP_OK) return rc;
+    }
+    uint32_t w = 0;
+    MP_CUDA(cudaMemcpyAsync(&w, word, sizeof(w), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (!w) return MP_OK;
+    MP_CUDA(cudaMemsetAsync(word, 0, sizeof(w), s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (w & mpb::kDevErrSpin)
+        return fail(MP_ERR_SPIN_LIMIT, "the scan's look-back wait gave up: its output is wrong (bits 0x%x)", w);
+    return fail(MP_ERR_DEVICE, "scan error word 0x%x", w);
 }
 
 }  // extern "C"

@@ -10,6 +10,7 @@
 
 #include "../../include/mtlphys_b200.h"
 #include "pbf_device.cuh"
+#include "pbf_kernels.h"
 
 namespace mpb {
 
@@ -23,6 +24,16 @@ const char* last_error();
         if (e_ != cudaSuccess)                                                                 \
             return ::mpb::fail(e_ == cudaErrorMemoryAllocation ? MP_ERR_OUT_OF_MEMORY : MP_ERR_CUDA, \
                                "%s: %s", #call, cudaGetErrorString(e_));                       \
+    } while (0)
+
+// Device allocation through the installed allocator (dev_alloc): returns
+// from the calling function with the status on failure.
+#define MP_ALLOC(ptr, bytes, device)                                                           \
+    do {                                                                                       \
+        void* p_ = nullptr;                                                                    \
+        const int rc_ = ::mpb::dev_alloc(&p_, (bytes), (device));                              \
+        if (rc_ != MP_OK) return rc_;                                                          \
+        (ptr) = static_cast<decltype(ptr)>(p_);                                                \
     } while (0)
 
 // Makes `dev` current for the scope and restores the previous device.

@@ -11,9 +11,10 @@
 // Scenes' particles and slots are contiguous ranges of the global arrays, and
 // each scene's boxes are laid end to end in the global cell arrays.
 //
-// Phases of one step, separated by a grid-wide barrier (bounded spin: on
-// expiry the kernel sets MP_DEVERR_SPIN_LIMIT and carries on instead of
-// hanging):
+// Phases of one step, separated by a grid-wide barrier (bounded spin: a
+// block that gives up sets MP_DEVERR_SPIN_LIMIT and an abort flag, and every
+// block leaves the launch at its next barrier, so no phase ever runs on the
+// incomplete output of an earlier one):
 //   0  per scene: reset the bounding box, advance the sphere
 //   1  per particle: predict, dense cell -> scene bounding box (atomics,
 //      reduced per warp first)
@@ -32,34 +33,50 @@
 namespace mpb {
 namespace {
 
-constexpr uint32_t kBarrierSpinLimit = 1u << 24;
 constexpr uint32_t kScanItems = 8;  // per thread and tile in phase 4
 
 // Grid-wide barrier with a generation counter.  Every block calls it the same
-// number of times; the wait is bounded.
-__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned* gen, uint32_t* err) {
+// number of times.  The wait is bounded: a block that waits more than
+// a.spin_limit polls sets the error bit and the abort flag.  Returns false
+// (to every thread of the block) when the launch is aborted, by this block or
+// another one; the block must then return.  A barrier only completes once
+// every block has arrived, i.e. finished the phase before it, so a block that
+// returns true works on complete data; a block that left early never
+// arrives at the next barrier, so nobody passes that one.
+__device__ __forceinline__ bool grid_barrier(const BatchArgs& a, int* s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = gen;
+        volatile unsigned* vgen = a.bar_gen;
+        volatile uint32_t* vabort = a.abort;
         const unsigned g = *vgen;
         __threadfence();
-        if (atomicAdd(count, 1u) + 1u == gridDim.x) {
-            atomicExch(count, 0u);
+        int ok = 1;
+        if (atomicAdd(a.bar_count, 1u) + 1u == gridDim.x + a.bar_extra) {
+            atomicExch(a.bar_count, 0u);
             __threadfence();
-            atomicAdd(gen, 1u);
+            atomicAdd(a.bar_gen, 1u);
         } else {
             uint32_t spins = 0;
             while (*vgen == g) {
-                if (++spins > kBarrierSpinLimit) {
-                    atomicOr(err, kDevErrSpin);
+                if (*vabort) {
+                    ok = 0;
+                    break;
+                }
+                if (++spins > a.spin_limit) {
+                    atomicOr(a.err, kDevErrSpin);
+                    atomicExch(a.abort, 1u);
+                    ok = 0;
                     break;
                 }
                 __nanosleep(64);
             }
         }
+        if (ok && *vabort) ok = 0;
         __threadfence();
+        *s_ok = ok;
     }
     __syncthreads();
+    return *s_ok != 0;
 }
 
 template <uint32_t BS>
@@ -103,7 +120,14 @@ constexpr int batch_min_blocks() {
 template <uint32_t BS>
 __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(BatchArgs a) {
     __shared__ uint32_t s_warp[BS / 32 + 1];
+    __shared__ int s_ok;
     const uint32_t gtid = blockIdx.x * BS + threadIdx.x;
+    // an earlier launch gave up on a barrier and left the barrier counter
+    // mid-count: do nothing until the host has re-armed the batch
+    if (*static_cast<volatile uint32_t*>(a.abort)) {
+        if (gtid == 0) atomicOr(a.err, kDevErrSpin);
+        return;
+    }
     const uint32_t gsize = gridDim.x * BS;
     const uint32_t pb = a.p_begin, pe = a.p_end;
     // loops over particles run in whole warps (warp-level operations inside)
@@ -118,7 +142,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
         if (sc[s].c.sphere) sphere_advance(sc[s].c, &sc[s].sphere);
     }
     if (gtid == 0) *a.long_count = 0;
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
 
     // 1: predict + dense cell of the predicted position -> scene bounding box
     for (uint32_t i = pb + gtid; i < pe_round; i += gsize) {
@@ -149,7 +173,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
             }
         }
     }
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
 
     // 2: sub-grid of every scene and its offset in the cell arrays
     if (blockIdx.x == 0) {
@@ -181,7 +205,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
         }
         if (threadIdx.x == 0) *a.total_cells = running;
     }
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
 
     // 3: cell id inside the scene's box + warp-aggregated count
     if (a.rec.scenes)
@@ -204,7 +228,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
         count_cell(active, cell, a.counts, &rank);
         if (active) a.off[i] = rank;
     }
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
 
     // 4: exclusive scan of counts[0, ncells] into cstart (counts left zero)
     const uint32_t len = cells_ok ? ncells + 1u : 0u;
@@ -220,7 +244,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
         block_exclusive_scan<BS>(sum, s_warp, total);
         if (threadIdx.x == 0) a.tile_sums[t] = total;
     }
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
     if (blockIdx.x == 0) {
         // slots of this launch start at its first particle (a scene's range
         // in serial mode)
@@ -234,7 +258,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
             running += total;
         }
     }
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         // each thread owns kScanItems consecutive items of the tile
         uint32_t v[kScanItems], sum = 0;
@@ -254,17 +278,17 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
                 run += v[k];
             }
     }
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
 
     // 5: scatter; 6: stable re-rank + gather; 7: long segments
     if (cells_ok)
         for (uint32_t i = pb + gtid; i < pe; i += gsize) scatter_item(i, a.hash, a.off, a.cstart, a.tmp);
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
     if (cells_ok)
         for (uint32_t s = pb + gtid; s < pe; s += gsize)
             sort_gather_item(s, a.tmp, a.hash, a.cstart, a.pos, a.sidx, a.sorted_a, a.long_list,
                              a.long_count);
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
     {
         const uint32_t nl = cells_ok ? *a.long_count : 0u;
         for (uint32_t li = blockIdx.x; li < nl; li += gridDim.x) {
@@ -274,7 +298,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
                          s_warp);
         }
     }
-    grid_barrier(a.bar_count, a.bar_gen, a.err);
+    if (!grid_barrier(a, &s_ok)) return;
 
     // 8+: solver
     const RowMasks rm{a.row_masks, a.mask_overflow, a.mask_stride};
@@ -282,7 +306,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
     if (a.iterations == 0) {
         for (uint32_t s = pb + gtid; s < pe; s += gsize)
             count_neighbors_item(sc[a.scene_of[s]].c, s, a.sorted_a, a.cstart, a.sidx, a.ncount);
-        grid_barrier(a.bar_count, a.bar_gen, a.err);
+        if (!grid_barrier(a, &s_ok)) return;
         for (uint32_t s = pb + gtid; s < pe; s += gsize)
             finalize_sorted_item(sc[a.scene_of[s]].c, s, a.sorted_a, a.sidx, a.pos, a.vel, a.prev,
                                  a.ncount, a.foam, a.err);
@@ -314,7 +338,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
                 lambda_item<false>(c, s, a.sorted_a, lam_out, a.scell, a.cstart, a.sidx, a.lambdas, rmi);
             }
         }
-        grid_barrier(a.bar_count, a.bar_gen, a.err);
+        if (!grid_barrier(a, &s_ok)) return;
         for (uint32_t s = pb + gtid; s < pe; s += gsize) {
             const SceneDev& sd = sc[a.scene_of[s]];
             if (last)
@@ -324,7 +348,7 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
                 delta_item<false>(sd.c, s, lam_out, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
                                   a.pos, a.vel, a.prev, a.ncount, a.foam, a.err, rmi, drec);
         }
-        if (!last) grid_barrier(a.bar_count, a.bar_gen, a.err);
+        if (!last && !grid_barrier(a, &s_ok)) return;
     }
 }
 

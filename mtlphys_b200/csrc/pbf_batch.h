@@ -49,6 +49,14 @@ struct BatchArgs {
     uint32_t* total_cells;
     unsigned *bar_count, *bar_gen;
     uint32_t* err;
+    // Bounded grid barrier: a block waits at most spin_limit polls.  One
+    // that gives up sets kDevErrSpin and *abort, and every block then leaves
+    // the launch at its next barrier; a launch that starts with *abort set
+    // does nothing (the host clears it in mp_batch_check_errors).
+    // bar_extra (a test hook, normally 0) makes every barrier wait for that
+    // many more blocks than the launch has, so that each wait runs out.
+    uint32_t* abort;
+    uint32_t spin_limit, bar_extra;
     BatchRecord rec;
 };
 

@@ -21,8 +21,6 @@
 namespace mpb {
 namespace {
 
-constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait (~0.1-1 s)
-
 // predictPositions (Constraints.metal:54-66) + hashCells (Spatial.metal:49-57)
 // + countCells (Spatial.metal:63-70) in one pass.
 __global__ void __launch_bounds__(256)
@@ -101,7 +99,7 @@ __device__ __forceinline__ void store4(uint32_t* out, uint32_t idx, uint32_t n, 
 template <bool VEC>
 __global__ void __launch_bounds__(kScanThreads)
 k_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status,
-       unsigned long long* ticket, uint32_t tiles, int zero_input, uint32_t* err) {
+       unsigned long long* ticket, uint32_t tiles, int zero_input, uint32_t* err, uint32_t spin_limit) {
     __shared__ uint32_t s_tile, s_tag, s_warp[kScanThreads / 32], s_excl;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
@@ -173,7 +171,7 @@ k_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status
                     excl += warp_sum(val);
                     base -= 32;
                 } else {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > spin_limit) {
                         if (lane == 0) atomicOr(err, kDevErrSpin);
                         break;
                     }
@@ -247,11 +245,12 @@ cudaError_t launch_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned 
                         cudaStream_t s, KernelTimer* t) {
     if (n == 0) return cudaSuccess;
     const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0;
+    const uint32_t spins = scan_spin_limit();
     tbegin(t, s);
     if (vec)
-        k_scan<true><<<tiles, kScanThreads, 0, s>>>(in, out, n, status, ticket, tiles, zero_input, err);
+        k_scan<true><<<tiles, kScanThreads, 0, s>>>(in, out, n, status, ticket, tiles, zero_input, err, spins);
     else
-        k_scan<false><<<tiles, kScanThreads, 0, s>>>(in, out, n, status, ticket, tiles, zero_input, err);
+        k_scan<false><<<tiles, kScanThreads, 0, s>>>(in, out, n, status, ticket, tiles, zero_input, err, spins);
     tend(t, "scan", s);
     return cudaGetLastError();
 }

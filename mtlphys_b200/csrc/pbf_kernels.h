@@ -53,9 +53,28 @@ struct KernelTimer {
     virtual ~KernelTimer() = default;
 };
 
+// Bounds, in polls, of the device-side waits (the scan's look-back, the batch
+// kernel's grid barrier).  mp_set_spin_limit() changes them process-wide;
+// launchers read them when they enqueue a kernel, and engines and batches
+// re-capture their CUDA graphs when spin_limit_epoch() has moved on.
+constexpr uint32_t kDefaultScanSpinLimit = 1u << 22;     // ~0.1-1 s of 32 ns naps
+constexpr uint32_t kDefaultBarrierSpinLimit = 1u << 24;  // ~1-10 s of 64 ns naps
+uint32_t scan_spin_limit();
+uint32_t barrier_spin_limit();
+uint32_t spin_limit_epoch();
+
+// Device memory of engines and batches: through the allocator installed
+// with mp_set_device_allocator (cudaMalloc/cudaFree by default).  Each block
+// is freed by the allocator that made it.  dev_alloc returns MP_OK or
+// MP_ERR_OUT_OF_MEMORY (message recorded).
+int dev_alloc(void** p, size_t bytes, int device);
+void dev_free(void* p);
+
 // Exclusive scan with decoupled look-back.  `status` holds `tiles` words and
 // `ticket` one word, both from an earlier call with the same tile count or
-// zeroed.  zero_input: write 0 over `in` after reading it.
+// zeroed.  zero_input: write 0 over `in` after reading it.  A look-back that
+// waits longer than scan_spin_limit() polls sets kDevErrSpin in *err and
+// gives that tile a wrong prefix (every write stays inside `out`).
 cudaError_t launch_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status,
                         unsigned long long* ticket, uint32_t tiles, bool zero_input, uint32_t* err,
                         cudaStream_t s, KernelTimer* t = nullptr);
@@ -102,5 +121,9 @@ cudaError_t launch_mouse_pulse(const MouseConsts& c, float4* vel, const float4* 
 
 // Sets the message mp_last_error() returns on this thread.
 void record_error(const char* msg);
+
+// Device address of the error word of mp_exclusive_scan_noalloc's static
+// scratch on the current device (MP_OK or an MP_ERR_* status).
+int noalloc_scan_error_word(cudaStream_t s, uint32_t** word);
 
 }  // namespace mpb

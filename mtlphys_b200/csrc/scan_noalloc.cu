@@ -12,7 +12,9 @@
 // The scratch (a tile ticket, an error word and one look-back descriptor per
 // 4096-element tile) lives in g_scan_scratch below: 33,024 bytes that every
 // GPU which loads the library holds until the process exits.  That bounds n
-// at kNoAllocMaxN = 2^24 elements.
+// at kNoAllocMaxN = 2^24 elements.  A look-back that gives up sets the error
+// word; mp_exclusive_scan_status(NULL, stream) reads and clears it (the next
+// call's own clearing of the header would otherwise hide it).
 #include "../../include/mtlphys_b200.h"
 
 #include <cuda_runtime.h>
@@ -41,11 +43,19 @@ int report(int code, const char* msg) {
 }
 
 // Device address of g_scan_scratch on the current device.  In host code the
-// symbol's name is only a host-side stand-in, so its address is looked up
-// once per device (with that device current) and cached.
-int scratch_address(int dev, void** out) {
+// symbol's name is only a host-side stand-in.  The address is looked up with
+// the device current on every call made outside stream capture (a few
+// microseconds), so it follows the module if the device was reset; a call
+// made while `s` is being captured uses the address of the last call outside
+// capture on this device, so the first call on a device must come before any
+// capture.
+int scratch_address(int dev, cudaStream_t s, void** out) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    const cudaError_t qe = cudaStreamIsCapturing(s, &cap);
+    if (qe != cudaSuccess) cudaGetLastError();  // drop the failed query's error; treat as capturing
+    const bool capturing = qe != cudaSuccess || cap != cudaStreamCaptureStatusNone;
     std::lock_guard<std::mutex> guard(g_lock);
-    if (!g_addr[dev]) {
+    if (!capturing) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
         if (e != cudaSuccess) {
@@ -55,8 +65,19 @@ int scratch_address(int dev, void** out) {
             return report(MP_ERR_CUDA, buf);
         }
         g_addr[dev] = p;
+    } else if (!g_addr[dev]) {
+        return report(MP_ERR_INVALID_ARGUMENT,
+                      "first mp_exclusive_scan_noalloc call on this device is inside a stream "
+                      "capture: make one call outside capture first");
     }
     *out = g_addr[dev];
+    return MP_OK;
+}
+
+int current_device(int* dev) {
+    const cudaError_t e = cudaGetDevice(dev);
+    if (e != cudaSuccess) return report(MP_ERR_CUDA, cudaGetErrorString(e));
+    if (*dev < 0 || *dev >= kMaxDevices) return report(MP_ERR_UNSUPPORTED, "device index too large");
     return MP_OK;
 }
 
@@ -75,14 +96,14 @@ extern "C" int mp_exclusive_scan_noalloc(const uint32_t* in, uint32_t* out, uint
         return report(MP_ERR_INVALID_ARGUMENT, buf);
     }
     int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return report(MP_ERR_CUDA, cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return report(MP_ERR_UNSUPPORTED, "device index too large");
+    int rc = current_device(&dev);
+    if (rc != MP_OK) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     void* base = nullptr;
-    const int rc = scratch_address(dev, &base);
+    rc = scratch_address(dev, s, &base);
     if (rc != MP_OK) return rc;
     const uint32_t tiles = mpb::scan_tiles_for(n);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
     // The array keeps the previous call's ticket and descriptors: clear the
     // header and the descriptors this call uses.
     e = cudaMemsetAsync(base, 0, (kHeaderWords + size_t(tiles)) * sizeof(unsigned long long), s);
@@ -91,5 +112,17 @@ extern "C" int mp_exclusive_scan_noalloc(const uint32_t* in, uint32_t* out, uint
     e = mpb::launch_scan(in, out, n, words + kHeaderWords, words, tiles, false,
                          reinterpret_cast<uint32_t*>(words + 1), s);
     if (e != cudaSuccess) return report(MP_ERR_CUDA, cudaGetErrorString(e));
+    return MP_OK;
+}
+
+// The error word (words[1]) of the static scratch, for mp_exclusive_scan_status.
+int mpb::noalloc_scan_error_word(cudaStream_t s, uint32_t** word) {
+    int dev = -1;
+    int rc = current_device(&dev);
+    if (rc != MP_OK) return rc;
+    void* base = nullptr;
+    rc = scratch_address(dev, s, &base);
+    if (rc != MP_OK) return rc;
+    *word = reinterpret_cast<uint32_t*>(static_cast<unsigned long long*>(base) + 1);
     return MP_OK;
 }

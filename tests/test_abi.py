@@ -84,3 +84,14 @@ def test_last_error_starts_empty_and_null_args_are_rejected():
     assert lib.mp_default_params(None) == _abi.MP_ERR_INVALID_ARGUMENT
     assert b"NULL" in lib.mp_last_error()
     assert lib.mp_engine_destroy(None) == _abi.MP_OK
+
+
+def test_failure_hooks_are_host_calls():
+    """mp_set_spin_limit and mp_set_device_allocator need no GPU; an
+    allocator without a free function is refused."""
+    lib = _abi.load()
+    assert lib.mp_set_spin_limit(1000) == _abi.MP_OK
+    assert lib.mp_set_spin_limit(0) == _abi.MP_OK
+    alloc = _abi.DEVICE_ALLOC_FN(lambda pp, n, dev, user: 1)
+    assert lib.mp_set_device_allocator(C.cast(alloc, C.c_void_p), None, None) == _abi.MP_ERR_INVALID_ARGUMENT
+    assert lib.mp_set_device_allocator(None, None, None) == _abi.MP_OK
