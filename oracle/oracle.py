@@ -86,6 +86,8 @@ def lib() -> C.CDLL:
         L.or_step.argtypes = [C.POINTER(PBFParams), C.c_float, C.c_uint32, _F, _F, C.c_void_p,
                               C.POINTER(StepOut)]
         L.or_step_f64.argtypes = [C.POINTER(PBFParams), C.c_double, C.c_uint32, _D, _D, C.c_void_p]
+        L.or_plant_fault.argtypes = [C.c_int]
+        L.or_plant_fault.restype = None
         L.or_set_threads.argtypes = [C.c_int]
         L.or_set_threads.restype = None
         L.or_get_threads.restype = C.c_int
@@ -242,6 +244,21 @@ def step_f64(p: PBFParams, dt: float, pos3, vel3, sphere=None) -> None:
     rc = lib().or_step_f64(C.byref(as_params(p)), C.c_double(dt), len(pos3), pos3, vel3, _ptr(sph))
     if rc != 0:
         raise ValueError(f"or_step_f64 failed ({rc})")
+
+
+class planted_fault:
+    """Context manager: the oracle's step runs with deliberate mistake
+    `which` (see or_plant_fault), so a test can show a check rejects it."""
+
+    def __init__(self, which: int):
+        self.which = which
+
+    def __enter__(self):
+        lib().or_plant_fault(self.which)
+        return self
+
+    def __exit__(self, *exc):
+        lib().or_plant_fault(0)
 
 
 def set_threads(n: int) -> None:

@@ -186,6 +186,10 @@ void sphere_advance(const Consts& c, double dt, double* s) {
     }
 }
 
+// A deliberate mistake the tests plant here, on the CPU, to show that the
+// parity checks catch it (or_plant_fault); 0 = none.
+int g_planted_fault = 0;
+
 // Metal's clamp(x, lo, hi) = fmin(fmax(x, lo), hi): a NaN coordinate goes to
 // the lower bound.
 inline double clampd(double x, double lo, double hi) { return std::fmin(std::fmax(x, lo), hi); }
@@ -240,10 +244,16 @@ int step_core(const mp_pbf_params* p, double dt, uint32_t n, const V3* pos, cons
             const V3 pi = cur[s];
             int cc[3];
             cell_coord_iter(g, pi, cc);
-            double dens = poly6(0.0, c), gsq = 0.0;
+            // planted fault 1: the self term W(0) only when the particle's own
+            // slot lies in the stencil of its current cell
+            const bool self_in_stencil_only = g_planted_fault == 1;
+            double dens = self_in_stencil_only ? 0.0 : poly6(0.0, c), gsq = 0.0;
             V3 gs = {0, 0, 0};
             for_stencil(g, cc, cell_start.data(), [&](uint32_t k) {
-                if (k == uint32_t(s)) return;
+                if (k == uint32_t(s)) {
+                    if (self_in_stencil_only) dens += poly6(0.0, c);
+                    return;
+                }
                 const V3 r = pi - cur[k];
                 const double r2 = dot(r, r);
                 if (r2 >= c.h2) return;
@@ -622,6 +632,8 @@ int or_step_f64(const mp_pbf_params* p, double dt, uint32_t n, double* pos3, dou
     std::memcpy(vel3, vo.data(), sizeof(V3) * n);
     return 0;
 }
+
+void or_plant_fault(int which) { g_planted_fault = which; }
 
 void or_set_threads(int n) {
 #ifdef _OPENMP

@@ -111,6 +111,11 @@ int or_step_f64(const mp_pbf_params* p, double dt, uint32_t n, double* pos3, dou
                 double* sphere);
 
 /* Number of OpenMP threads the oracle uses (0 -> runtime default). */
+/* Test hook: plant a deliberate mistake in the oracle's step so that a test
+ * can show the parity checks reject it.  1: the density starts at the
+ * particle's own W(0) only when its slot lies in the stencil of its current
+ * cell (instead of always, Constraints.metal:99-108).  0: none. */
+void or_plant_fault(int which);
 void or_set_threads(int n);
 int  or_get_threads(void);
 

@@ -265,3 +265,20 @@ def test_mouse_pulse_matches_the_reference_shader():
     np.testing.assert_allclose(v, g["mouse/vel"], rtol=1e-6, atol=1e-6)
     moved = np.abs(g["mouse/vel"] - g["mouse/vel_in"]).max(1) > 0
     assert 10 < moved.sum() < len(moved)  # the case exercises both branches
+
+
+def test_planted_self_density_fault_changes_the_oracle():
+    """The mistake the GPU parity tests plant in the oracle (or_plant_fault 1:
+    the density starts at W(0) only when the particle's own slot lies in the
+    stencil of its current cell) really changes the step where particles
+    drift two cells within it (the exploding clumps of a random cloud), and
+    the context manager takes it out again."""
+    p = ref_params()
+    pos, vel = random_scene(3, 3000)
+    good = O.step(p, 1.0 / 240.0, pos, vel)["pos"]
+    with O.planted_fault(1):
+        bad = O.step(p, 1.0 / 240.0, pos, vel)["pos"]
+    again = O.step(p, 1.0 / 240.0, pos, vel)["pos"]
+    moved = np.abs(bad - good).max(axis=1)
+    assert (moved > 1e-4).sum() >= 10, (moved > 1e-4).sum()
+    assert np.array_equal(good, again)
