@@ -147,12 +147,17 @@ struct mp_batch {
         if (adj_block) return MP_OK;
         const size_t cap = cap_slots(), v4 = al(cap * 16), u = al(cap * 4);
         const size_t gbytes = al(sizeof(double) * kGradStride * std::max<uint32_t>(S, 1u));
-        const size_t total = 8 * v4 + 5 * u + gbytes;
+        // one-way pair inboxes and the overflow list; FP64 per-slot scene-gradient shares
+        const size_t inbox = kInbox * (u + v4);
+        const size_t ovf = 2 * al(4 * size_t(kInboxOverflow)) + al(16 * size_t(kInboxOverflow)) + 256;
+        const size_t accs = al(cap * 8) + al(cap * 32);
+        const size_t total = 8 * v4 + 6 * u + gbytes + inbox + ovf + accs;
         MP_ALLOC(adj_block, total, device);
         MP_CUDA(cudaMemset(adj_block, 0, total));
         char* p = static_cast<char*>(adj_block);
         auto v = [&]() { float4* r = reinterpret_cast<float4*>(p); p += v4; return r; };
         auto w = [&]() { char* r = p; p += u; return r; };
+        auto take = [&](size_t bytes) { char* r = p; p += al(bytes); return r; };
         adj = AdjArgs{};
         adj.pbar = v();
         adj.qbar = v();
@@ -167,6 +172,16 @@ struct mp_batch {
         adj.lam_extra = reinterpret_cast<float*>(w());
         adj.ccur = reinterpret_cast<uint32_t*>(w());
         adj.cpred = reinterpret_cast<uint32_t*>(w());
+        adj.inbox_count = reinterpret_cast<uint32_t*>(w());
+        adj.inbox_src = reinterpret_cast<uint32_t*>(take(kInbox * u));
+        adj.inbox_val = reinterpret_cast<float4*>(take(kInbox * v4));
+        adj.ovf_count = reinterpret_cast<uint32_t*>(take(256));
+        adj.ovf_dst = reinterpret_cast<uint32_t*>(take(4 * size_t(kInboxOverflow)));
+        adj.ovf_src = reinterpret_cast<uint32_t*>(take(4 * size_t(kInboxOverflow)));
+        adj.ovf_val = reinterpret_cast<float4*>(take(16 * size_t(kInboxOverflow)));
+        adj.kacc = reinterpret_cast<double*>(take(cap * 8));
+        adj.sacc = reinterpret_cast<double4*>(take(cap * 32));
+        adj.err = a.err;
         adj.grads = reinterpret_cast<double*>(p);
         adj.scene_of = a.scene_of;
         adj.n = N;
@@ -836,6 +851,9 @@ int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel,
     if (dvel) MP_CUDA(cudaMemcpyAsync(ad.vbar, dvel, v4, cudaMemcpyDeviceToDevice, st));
     else MP_CUDA(cudaMemsetAsync(ad.vbar, 0, v4, st));
     MP_CUDA(cudaMemsetAsync(ad.grads, 0, sizeof(double) * kGradStride * b->S, st));
+    MP_CUDA(cudaMemsetAsync(ad.kacc, 0, sizeof(double) * b->N, st));
+    MP_CUDA(cudaMemsetAsync(ad.sacc, 0, sizeof(double4) * b->N, st));
+    MP_CUDA(cudaMemsetAsync(ad.inbox_count, 0, sizeof(uint32_t) * b->N, st));
     const mp_batch::Saved& fin = b->ckpts[nck];
     rc = b->save(fin, st);
     for (uint32_t seg = nck; rc == MP_OK && seg-- > 0;) {
@@ -846,6 +864,12 @@ int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel,
             const float4* x1 = t + 1 == t1 ? b->a.pos : b->slots[t + 1 - t0].x0;
             rc = b->enqueue_adjoint(t - t0, x1, st);
         }
+    }
+    if (rc == MP_OK) {  // dL/dk of every scene from the per-slot shares
+        AdjArgs fa = ad;
+        fa.t.scenes = b->slots[0].rec.scenes;
+        const cudaError_t e = launch_adjoint_finish(fa, st);
+        if (e != cudaSuccess) rc = fail(MP_ERR_CUDA, "adjoint finish launch: %s", cudaGetErrorString(e));
     }
     if (rc == MP_OK) rc = b->restore(fin, st);
     if (rc != MP_OK) return rc;
@@ -859,7 +883,7 @@ int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel,
 
 uint32_t mp_batch_rollout_launch_count(const mp_batch* b, uint32_t steps) {
     if (!b || b->N == 0) return 0;
-    return steps * (1u + adjoint_launch_count(b->iterations));
+    return steps * (1u + adjoint_launch_count(b->iterations)) + (steps ? 1u : 0u);
 }
 
 size_t mp_batch_snapshot_size(const mp_batch* b) {

@@ -21,11 +21,16 @@
 //
 // The pair sweeps walk exactly the pairs of the forward iteration: the row
 // masks its lambda pass recorded (long rows distance-tested past their first
-// 32 candidates, as the forward delta pass does).  The reference's neighbour search makes those lists
-// asymmetric once particles leave their predicted cells (j is in i's list iff
-// j's predicted cell is next to i's current cell), so each pair term of i's
-// list is delivered to j by j's own sweep when i is in j's list too (a test
-// on the two cells), and by an atomic add otherwise.
+// 32 candidates, as the forward delta pass does).  The reference's neighbour
+// search makes those lists asymmetric once particles leave their predicted
+// cells (j is in i's list iff j's predicted cell is next to i's current
+// cell), so each pair term of i's list is delivered to j by j's own sweep
+// when i is in j's list too (a test on the two cells).  Otherwise (a one-way
+// pair, ~0.4% of pairs in a 60-step cube drop) i posts the term to j's inbox
+// and a delivery kernel adds j's posts in ascending order of the sender's
+// slot.  The scene gradients (dL/dk, the sphere's center and radius) are
+// accumulated per slot and summed per scene in a fixed order.  Nothing is
+// added with float atomics, so the gradients are the same bytes on every run.
 #include "pbf_adjoint.h"
 #include "pbf_items.cuh"
 
@@ -76,26 +81,24 @@ __device__ __forceinline__ float pow_u(float x, uint32_t n) {
     return r;
 }
 
-// Sum of v over the lanes of each scene in the warp, added to
-// grads[scene * kGradStride + field] in FP64.  Every lane of the warp calls it.
-__device__ __forceinline__ void add_per_scene(bool active, uint32_t scene, double v, double* grads,
-                                              uint32_t field) {
-    const unsigned act = __ballot_sync(kFull, active);
-    if (!active) return;
-    const unsigned peers = __match_any_sync(act, scene);
-    if (peers == kFull) {  // one scene in the whole warp (the usual case)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&grads[size_t(scene) * kGradStride + field], v);
-    } else if (v != 0.0) {
-        atomicAdd(&grads[size_t(scene) * kGradStride + field], v);
+// Posts the term v that sender slot `from` owes receiver slot `to` (a
+// one-way pair): into one of the receiver's kInbox entries, or the shared
+// overflow list; a post that fits in neither sets kDevErrIndex.
+__device__ __forceinline__ void post(const AdjArgs& a, uint32_t to, uint32_t from, const float4& v) {
+    const uint32_t e = atomicAdd(&a.inbox_count[to], 1u);
+    if (e < kInbox) {
+        a.inbox_src[size_t(e) * a.stride + to] = from;
+        a.inbox_val[size_t(e) * a.stride + to] = v;
+        return;
     }
-}
-
-__device__ __forceinline__ void atomic_add3(float4* p, float x, float y, float z) {
-    atomicAdd(&p->x, x);
-    atomicAdd(&p->y, y);
-    atomicAdd(&p->z, z);
+    const uint32_t o = atomicAdd(a.ovf_count, 1u);
+    if (o < kInboxOverflow) {
+        a.ovf_dst[o] = to;
+        a.ovf_src[o] = from;
+        a.ovf_val[o] = v;
+    } else {
+        atomicOr(a.err, kDevErrIndex);
+    }
 }
 
 // ---- finalize --------------------------------------------------------------
@@ -147,9 +150,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_finalize(AdjArgs a) {
 // `it`; records the iterate's current cell for the pair sweeps.
 __global__ void __launch_bounds__(kBlock) k_adj_pre(AdjArgs a, uint32_t it) {
     const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
+    if (s == 0) *a.ovf_count = 0;  // the delta sweep posts into an empty list
     if (s >= a.n) return;
-    const uint32_t scene = a.scene_of[s];
-    const SceneDev& sd = a.t.scenes[scene];
+    const SceneDev& sd = a.t.scenes[a.scene_of[s]];
     const StepConsts& c = sd.c;
     const size_t off = size_t(it) * a.stride;
     const float4 l = a.t.lam[off + s];
@@ -196,9 +199,12 @@ __global__ void __launch_bounds__(kBlock) k_adj_pre(AdjArgs a, uint32_t it) {
                 cb[k] = pb[k] - eb[k];
             }
             const double rb = e[0] * pb[0] + e[1] * pb[1] + e[2] * pb[2];
-            double* g = a.grads + size_t(scene) * kGradStride;
-            for (int k = 0; k < 3; ++k) atomicAdd(&g[kGradCenter + k], cb[k]);
-            atomicAdd(&g[kGradRadius], rb);
+            double4 sa = a.sacc[s];  // this slot's share of the step's sphere gradient
+            sa.x += cb[0];
+            sa.y += cb[1];
+            sa.z += cb[2];
+            sa.w += rb;
+            a.sacc[s] = sa;
             for (int k = 0; k < 3; ++k) pb[k] = float(eb[k]);
         }
     }
@@ -232,12 +238,9 @@ constexpr int kSweepMinBlocks = MPB_ADJ_SWEEP_MIN_BLOCKS;
 
 __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_delta(AdjArgs a, uint32_t it) {
     const uint32_t m = blockIdx.x * kBlock + threadIdx.x;
-    const bool active = m < a.n;
-    uint32_t scene = 0;
     float kb = 0.0f;
-    if (active) {
-        scene = a.scene_of[m];
-        const StepConsts& c = a.t.scenes[scene].c;
+    if (m < a.n) {
+        const StepConsts& c = a.t.scenes[a.scene_of[m]].c;
         const size_t off = size_t(it) * a.stride;
         const float4* src = a.t.lam + off;
         const float4 l = src[m];
@@ -292,8 +295,8 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_delta(AdjArgs a
                 px += vx;
                 py += vy;
                 pz += vz;
-                atomicAdd(&a.lam_extra[k], gdm * c.inv_rho0);
-                atomic_add3(&a.p_extra[k], -vx * c.inv_rho0, -vy * c.inv_rho0, -vz * c.inv_rho0);
+                post(a, k, m,
+                     make_float4(-vx * c.inv_rho0, -vy * c.inv_rho0, -vz * c.inv_rho0, gdm * c.inv_rho0));
             }
         };
         const uint32_t ms = a.mask_stride;
@@ -307,8 +310,8 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_delta(AdjArgs a
         const float D = ir * ir * (gx * gx + gy * gy + gz * gz + gsq) + c.eps;
         a.gd[m] = make_float4(gx, gy, gz, D);
         kb *= ir;
+        a.kacc[m] += double(kb);  // this slot's share of dL/dk
     }
-    add_per_scene(active, scene, double(kb), a.grads, kGradK);
 }
 
 // dL/d(density sum, gradient sum, squared-gradient sum) of each particle's
@@ -317,6 +320,7 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_delta(AdjArgs a
 //   Gbar = 2 Dbar G / rho0^2, Qbar = Dbar / rho0^2.
 __global__ void __launch_bounds__(kBlock) k_adj_lbar(AdjArgs a, uint32_t it) {
     const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
+    if (s == 0) *a.ovf_count = 0;  // the lambda sweep posts into an empty list
     if (s >= a.n) return;
     const StepConsts& c = a.t.scenes[a.scene_of[s]].c;
     const float lb = a.lam_part[s] + a.lam_extra[s];
@@ -373,7 +377,7 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_lambda(AdjArgs 
             px += vx;
             py += vy;
             pz += vz;
-            atomic_add3(&a.p_extra[k], -vx, -vy, -vz);
+            post(a, k, m, make_float4(-vx, -vy, -vz, 0.0f));
         }
     };
     const uint32_t ms = a.mask_stride;
@@ -381,6 +385,111 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) k_adj_lambda(AdjArgs 
                       const_cast<uint32_t*>(a.t.overflow) + size_t(it) * ms, ms};
     masked_pairs(c, src, a.t.cstart, rm, m, l, ax, ay, az, cx, cy, cz, body);
     a.pbar[m] = make_float4(px, py, pz, 0.0f);
+}
+
+// ---- delivery of one-way pair terms, scene sums ----------------------------------
+
+// Adds every post of receiver slot j in ascending order of the sender's slot
+// (a sender posts to a receiver at most once per sweep): p_extra += the
+// xyz sums, and with LAMBDA lam_extra += the w sum.  Posts beyond the inbox
+// are looked up in the overflow list.
+template <bool LAMBDA>
+__global__ void __launch_bounds__(kBlock) k_adj_deliver(AdjArgs a) {
+    const uint32_t j = blockIdx.x * kBlock + threadIdx.x;
+    if (j >= a.n) return;
+    const uint32_t cnt = a.inbox_count[j];
+    if (cnt == 0) return;
+    a.inbox_count[j] = 0;
+    const uint32_t nin = min(cnt, kInbox);
+    const uint32_t novf = cnt > kInbox ? min(*a.ovf_count, kInboxOverflow) : 0u;
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f, sw = 0.0f;
+    uint32_t last = 0;
+    for (uint32_t done = 0; done < cnt; ++done) {
+        uint32_t best = 0xffffffffu;
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (uint32_t e = 0; e < nin; ++e) {
+            const uint32_t src = a.inbox_src[size_t(e) * a.stride + j];
+            if ((done == 0 || src > last) && src < best) {
+                best = src;
+                v = a.inbox_val[size_t(e) * a.stride + j];
+            }
+        }
+        for (uint32_t o = 0; o < novf; ++o) {
+            if (a.ovf_dst[o] != j) continue;
+            const uint32_t src = a.ovf_src[o];
+            if ((done == 0 || src > last) && src < best) {
+                best = src;
+                v = a.ovf_val[o];
+            }
+        }
+        if (best == 0xffffffffu) break;  // posts dropped with the overflow list full
+        sx += v.x;
+        sy += v.y;
+        sz += v.z;
+        sw += v.w;
+        last = best;
+    }
+    const float4 pe = a.p_extra[j];
+    a.p_extra[j] = make_float4(pe.x + sx, pe.y + sy, pe.z + sz, 0.0f);
+    if (LAMBDA) a.lam_extra[j] += sw;
+}
+
+// Fixed-order block sum of one double per thread (blockDim.x == kBlock).
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t w = kBlock / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// One block per scene: the step's sphere gradient, summed over the scene's
+// slots in a fixed order, is added to the scene's center / radius adjoint;
+// the per-slot accumulators are cleared.
+__global__ void __launch_bounds__(kBlock) k_adj_sphere_sum(AdjArgs a) {
+    __shared__ double sh[kBlock];
+    const SceneDev& sd = a.t.scenes[blockIdx.x];
+    if (!sd.c.sphere) return;  // only sphere scenes accumulate
+    const uint32_t p0 = sd.p0, n = sd.c.n;
+    double cx = 0.0, cy = 0.0, cz = 0.0, r = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += kBlock) {
+        const double4 v = a.sacc[p0 + i];
+        cx += v.x;
+        cy += v.y;
+        cz += v.z;
+        r += v.w;
+        a.sacc[p0 + i] = make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+    cx = block_sum(cx, sh);
+    cy = block_sum(cy, sh);
+    cz = block_sum(cz, sh);
+    r = block_sum(r, sh);
+    if (threadIdx.x == 0) {
+        double* g = a.grads + size_t(blockIdx.x) * kGradStride;
+        g[kGradCenter] += cx;
+        g[kGradCenter + 1] += cy;
+        g[kGradCenter + 2] += cz;
+        g[kGradRadius] += r;
+    }
+}
+
+// One block per scene: dL/dk = the sum of the per-slot accumulators over the
+// scene's slots (fixed order), which are cleared.
+__global__ void __launch_bounds__(kBlock) k_adj_k_sum(AdjArgs a) {
+    __shared__ double sh[kBlock];
+    const SceneDev& sd = a.t.scenes[blockIdx.x];
+    const uint32_t p0 = sd.p0, n = sd.c.n;
+    double k = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += kBlock) {
+        k += a.kacc[p0 + i];
+        a.kacc[p0 + i] = 0.0;
+    }
+    k = block_sum(k, sh);
+    if (threadIdx.x == 0) a.grads[size_t(blockIdx.x) * kGradStride + kGradK] = k;
 }
 
 // ---- predict, sphere ----------------------------------------------------------
@@ -452,14 +561,23 @@ cudaError_t launch_adjoint_step(const AdjArgs& a, cudaStream_t s) {
     for (uint32_t it = a.iterations; it-- > 0;) {
         k_adj_pre<<<grid, kBlock, 0, s>>>(a, it);
         k_adj_delta<<<grid, kBlock, 0, s>>>(a, it);
+        k_adj_deliver<true><<<grid, kBlock, 0, s>>>(a);
         k_adj_lbar<<<grid, kBlock, 0, s>>>(a, it);
         k_adj_lambda<<<grid, kBlock, 0, s>>>(a, it);
+        k_adj_deliver<false><<<grid, kBlock, 0, s>>>(a);
     }
     k_adj_predict<<<grid, kBlock, 0, s>>>(a);
+    if (a.nscenes) k_adj_sphere_sum<<<a.nscenes, kBlock, 0, s>>>(a);
     k_adj_sphere<<<cdiv(a.nscenes, 128), 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-uint32_t adjoint_launch_count(uint32_t iterations) { return 3u + 4u * iterations; }
+cudaError_t launch_adjoint_finish(const AdjArgs& a, cudaStream_t s) {
+    if (a.n == 0 || a.nscenes == 0) return cudaSuccess;
+    k_adj_k_sum<<<a.nscenes, kBlock, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+uint32_t adjoint_launch_count(uint32_t iterations) { return 4u + 6u * iterations; }
 
 }  // namespace mpb

@@ -32,6 +32,15 @@ struct AdjStep {
     const uint32_t* overflow;     // iterations x mask_stride: bit r set for a long row r
 };
 
+// Pair terms that a particle's sweep owes another particle whose own sweep
+// does not see the pair (one-way pairs) are posted to the receiver's inbox:
+// kInbox slots per receiver, then a shared overflow list.  A delivery kernel
+// then adds each receiver's posts in ascending order of the sender's slot,
+// so the sums do not depend on the order the posts arrived in (no float
+// atomics: two backward passes give the same bytes).
+constexpr uint32_t kInbox = 4;
+constexpr uint32_t kInboxOverflow = 1u << 16;  // posts beyond kInbox, all receivers together
+
 struct AdjArgs {
     AdjStep t;
     const uint32_t* scene_of;     // scene of every particle / slot
@@ -42,13 +51,30 @@ struct AdjArgs {
     float4 *pbar, *qbar, *dbar, *lbar, *gd, *p_extra;
     float *qsc, *lam_part, *lam_extra;
     uint32_t *ccur, *cpred;
+    // one-way pair posts: per receiver slot a count and kInbox (sender,
+    // value) entries (entry e of receiver j at e * stride + j), then the
+    // overflow list (receiver, sender, value) with its count
+    uint32_t *inbox_count, *inbox_src;
+    float4* inbox_val;
+    uint32_t *ovf_count, *ovf_dst, *ovf_src;
+    float4* ovf_val;
+    // per-slot FP64 accumulators of the scene gradients, reduced per scene in
+    // a fixed order: dL/dk (over the whole backward pass) and the sphere's
+    // center (xyz) and radius (w) (over one step)
+    double* kacc;
+    double4* sacc;
+    uint32_t* err;                // device error word (kDevErrIndex: a post was dropped)
     double* grads;                // nscenes x kGradStride
 };
 
 // Enqueue the reverse of one step: finalize, every solver iteration in
-// reverse order, predict, and the sphere kinematics.  p_extra and lam_extra
-// must be zero on entry (they are left zero).
+// reverse order, predict, and the sphere kinematics.  p_extra, lam_extra,
+// inbox_count and sacc must be zero on entry (they are left zero); kacc
+// accumulates.
 cudaError_t launch_adjoint_step(const AdjArgs& a, cudaStream_t s);
+// grads[scene][kGradK] = the sum of kacc over the scene's slots (fixed order);
+// kacc is cleared.
+cudaError_t launch_adjoint_finish(const AdjArgs& a, cudaStream_t s);
 
 // Kernel launches per reversed step.
 uint32_t adjoint_launch_count(uint32_t iterations);
