@@ -150,8 +150,11 @@ struct mp_batch {
         // one-way pair inboxes and the overflow list; FP64 per-slot scene-gradient shares
         const size_t inbox = kInbox * (u + v4);
         const size_t ovf = 2 * al(4 * size_t(kInboxOverflow)) + al(16 * size_t(kInboxOverflow)) + 256;
-        const size_t accs = al(cap * 8) + al(cap * 32);
-        const size_t total = 8 * v4 + 6 * u + gbytes + inbox + ovf + accs;
+        uint32_t most = 1;
+        for (uint32_t c : counts) most = std::max(most, c);
+        const uint32_t chunks = (most + kSumChunk - 1) / kSumChunk;
+        const size_t accs = al(cap * 8) + al(cap * 32) + al(32 * size_t(chunks) * std::max<uint32_t>(S, 1u));
+        const size_t total = 8 * v4 + 7 * u + gbytes + inbox + ovf + accs;
         MP_ALLOC(adj_block, total, device);
         MP_CUDA(cudaMemset(adj_block, 0, total));
         char* p = static_cast<char*>(adj_block);
@@ -173,14 +176,18 @@ struct mp_batch {
         adj.ccur = reinterpret_cast<uint32_t*>(w());
         adj.cpred = reinterpret_cast<uint32_t*>(w());
         adj.inbox_count = reinterpret_cast<uint32_t*>(w());
+        adj.ovf_head = reinterpret_cast<uint32_t*>(w());
+        MP_CUDA(cudaMemset(adj.ovf_head, 0xff, 4 * cap));  // kNoPost
         adj.inbox_src = reinterpret_cast<uint32_t*>(take(kInbox * u));
         adj.inbox_val = reinterpret_cast<float4*>(take(kInbox * v4));
         adj.ovf_count = reinterpret_cast<uint32_t*>(take(256));
-        adj.ovf_dst = reinterpret_cast<uint32_t*>(take(4 * size_t(kInboxOverflow)));
         adj.ovf_src = reinterpret_cast<uint32_t*>(take(4 * size_t(kInboxOverflow)));
+        adj.ovf_next = reinterpret_cast<uint32_t*>(take(4 * size_t(kInboxOverflow)));
         adj.ovf_val = reinterpret_cast<float4*>(take(16 * size_t(kInboxOverflow)));
         adj.kacc = reinterpret_cast<double*>(take(cap * 8));
         adj.sacc = reinterpret_cast<double4*>(take(cap * 32));
+        adj.spart = reinterpret_cast<double4*>(take(32 * size_t(chunks) * std::max<uint32_t>(S, 1u)));
+        adj.sum_chunks = chunks;
         adj.err = a.err;
         adj.grads = reinterpret_cast<double*>(p);
         adj.scene_of = a.scene_of;
@@ -854,6 +861,7 @@ int mp_batch_rollout_backward(mp_batch* b, const float* dpos, const float* dvel,
     MP_CUDA(cudaMemsetAsync(ad.kacc, 0, sizeof(double) * b->N, st));
     MP_CUDA(cudaMemsetAsync(ad.sacc, 0, sizeof(double4) * b->N, st));
     MP_CUDA(cudaMemsetAsync(ad.inbox_count, 0, sizeof(uint32_t) * b->N, st));
+    MP_CUDA(cudaMemsetAsync(ad.ovf_head, 0xff, sizeof(uint32_t) * b->N, st));
     const mp_batch::Saved& fin = b->ckpts[nck];
     rc = b->save(fin, st);
     for (uint32_t seg = nck; rc == MP_OK && seg-- > 0;) {

@@ -82,8 +82,9 @@ __device__ __forceinline__ float pow_u(float x, uint32_t n) {
 }
 
 // Posts the term v that sender slot `from` owes receiver slot `to` (a
-// one-way pair): into one of the receiver's kInbox entries, or the shared
-// overflow list; a post that fits in neither sets kDevErrIndex.
+// one-way pair): into one of the receiver's kInbox entries, or a pooled
+// entry linked into the receiver's overflow list; a post that finds the pool
+// exhausted sets kDevErrIndex.
 __device__ __forceinline__ void post(const AdjArgs& a, uint32_t to, uint32_t from, const float4& v) {
     const uint32_t e = atomicAdd(&a.inbox_count[to], 1u);
     if (e < kInbox) {
@@ -93,9 +94,9 @@ __device__ __forceinline__ void post(const AdjArgs& a, uint32_t to, uint32_t fro
     }
     const uint32_t o = atomicAdd(a.ovf_count, 1u);
     if (o < kInboxOverflow) {
-        a.ovf_dst[o] = to;
         a.ovf_src[o] = from;
         a.ovf_val[o] = v;
+        a.ovf_next[o] = atomicExch(&a.ovf_head[to], o);
     } else {
         atomicOr(a.err, kDevErrIndex);
     }
@@ -401,7 +402,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_deliver(AdjArgs a) {
     if (cnt == 0) return;
     a.inbox_count[j] = 0;
     const uint32_t nin = min(cnt, kInbox);
-    const uint32_t novf = cnt > kInbox ? min(*a.ovf_count, kInboxOverflow) : 0u;
+    const uint32_t head = cnt > kInbox ? a.ovf_head[j] : kNoPost;
     float sx = 0.0f, sy = 0.0f, sz = 0.0f, sw = 0.0f;
     uint32_t last = 0;
     for (uint32_t done = 0; done < cnt; ++done) {
@@ -414,21 +415,21 @@ __global__ void __launch_bounds__(kBlock) k_adj_deliver(AdjArgs a) {
                 v = a.inbox_val[size_t(e) * a.stride + j];
             }
         }
-        for (uint32_t o = 0; o < novf; ++o) {
-            if (a.ovf_dst[o] != j) continue;
+        for (uint32_t o = head; o != kNoPost; o = a.ovf_next[o]) {
             const uint32_t src = a.ovf_src[o];
             if ((done == 0 || src > last) && src < best) {
                 best = src;
                 v = a.ovf_val[o];
             }
         }
-        if (best == 0xffffffffu) break;  // posts dropped with the overflow list full
+        if (best == 0xffffffffu) break;  // posts dropped with the pool exhausted
         sx += v.x;
         sy += v.y;
         sz += v.z;
         sw += v.w;
         last = best;
     }
+    if (head != kNoPost) a.ovf_head[j] = kNoPost;
     const float4 pe = a.p_extra[j];
     a.p_extra[j] = make_float4(pe.x + sx, pe.y + sy, pe.z + sz, 0.0f);
     if (LAMBDA) a.lam_extra[j] += sw;
@@ -447,34 +448,30 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return r;
 }
 
-// One block per scene: the step's sphere gradient, summed over the scene's
-// slots in a fixed order, is added to the scene's center / radius adjoint;
-// the per-slot accumulators are cleared.
+// Block (chunk, scene): the step's sphere gradient summed, in a fixed order,
+// over the chunk's kSumChunk slots of a sphere scene into spart; the per-slot
+// accumulators are cleared.  k_adj_sphere adds the chunks in order.
 __global__ void __launch_bounds__(kBlock) k_adj_sphere_sum(AdjArgs a) {
     __shared__ double sh[kBlock];
-    const SceneDev& sd = a.t.scenes[blockIdx.x];
+    const uint32_t chunk = blockIdx.x, sc = blockIdx.y;
+    const SceneDev& sd = a.t.scenes[sc];
     if (!sd.c.sphere) return;  // only sphere scenes accumulate
-    const uint32_t p0 = sd.p0, n = sd.c.n;
+    const uint32_t first = chunk * kSumChunk, n = sd.c.n;
+    const uint32_t end = min(n, first + kSumChunk);
     double cx = 0.0, cy = 0.0, cz = 0.0, r = 0.0;
-    for (uint32_t i = threadIdx.x; i < n; i += kBlock) {
-        const double4 v = a.sacc[p0 + i];
+    for (uint32_t i = first + threadIdx.x; i < end; i += kBlock) {
+        const double4 v = a.sacc[sd.p0 + i];
         cx += v.x;
         cy += v.y;
         cz += v.z;
         r += v.w;
-        a.sacc[p0 + i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        a.sacc[sd.p0 + i] = make_double4(0.0, 0.0, 0.0, 0.0);
     }
     cx = block_sum(cx, sh);
     cy = block_sum(cy, sh);
     cz = block_sum(cz, sh);
     r = block_sum(r, sh);
-    if (threadIdx.x == 0) {
-        double* g = a.grads + size_t(blockIdx.x) * kGradStride;
-        g[kGradCenter] += cx;
-        g[kGradCenter + 1] += cy;
-        g[kGradCenter + 2] += cz;
-        g[kGradRadius] += r;
-    }
+    if (threadIdx.x == 0) a.spart[size_t(sc) * a.sum_chunks + chunk] = make_double4(cx, cy, cz, r);
 }
 
 // One block per scene: dL/dk = the sum of the per-slot accumulators over the
@@ -514,6 +511,17 @@ __global__ void __launch_bounds__(128) k_adj_sphere(AdjArgs a) {
     if (sc >= a.nscenes) return;
     const StepConsts& c = a.t.scenes[sc].c;
     if (!c.sphere) return;
+    {  // this step's push terms, chunk by chunk in order (k_adj_sphere_sum)
+        double* g = a.grads + size_t(sc) * kGradStride;
+        const uint32_t chunks = (c.n + kSumChunk - 1) / kSumChunk;
+        for (uint32_t k = 0; k < chunks; ++k) {
+            const double4 v = a.spart[size_t(sc) * a.sum_chunks + k];
+            g[kGradCenter] += v.x;
+            g[kGradCenter + 1] += v.y;
+            g[kGradCenter + 2] += v.z;
+            g[kGradRadius] += v.w;
+        }
+    }
     const SphereState s0 = a.t.sphere0[sc];
     // forward branch decisions, as sphere_advance computes them
     float v[3] = {s0.v[0], __fadd_rn(s0.v[1], __fmul_rn(c.sph_gravity, c.dt)), s0.v[2]};
@@ -567,7 +575,7 @@ cudaError_t launch_adjoint_step(const AdjArgs& a, cudaStream_t s) {
         k_adj_deliver<false><<<grid, kBlock, 0, s>>>(a);
     }
     k_adj_predict<<<grid, kBlock, 0, s>>>(a);
-    if (a.nscenes) k_adj_sphere_sum<<<a.nscenes, kBlock, 0, s>>>(a);
+    if (a.nscenes && a.sum_chunks) k_adj_sphere_sum<<<dim3(a.sum_chunks, a.nscenes), kBlock, 0, s>>>(a);
     k_adj_sphere<<<cdiv(a.nscenes, 128), 128, 0, s>>>(a);
     return cudaGetLastError();
 }

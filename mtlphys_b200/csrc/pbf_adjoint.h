@@ -34,12 +34,16 @@ struct AdjStep {
 
 // Pair terms that a particle's sweep owes another particle whose own sweep
 // does not see the pair (one-way pairs) are posted to the receiver's inbox:
-// kInbox slots per receiver, then a shared overflow list.  A delivery kernel
-// then adds each receiver's posts in ascending order of the sender's slot,
-// so the sums do not depend on the order the posts arrived in (no float
-// atomics: two backward passes give the same bytes).
+// kInbox slots per receiver, then a shared pool of overflow entries linked
+// into a list per receiver.  A delivery kernel then adds each receiver's
+// posts in ascending order of the sender's slot, so the sums do not depend
+// on the order the posts arrived in (no float atomics: two backward passes
+// give the same bytes).
 constexpr uint32_t kInbox = 4;
-constexpr uint32_t kInboxOverflow = 1u << 16;  // posts beyond kInbox, all receivers together
+constexpr uint32_t kInboxOverflow = 1u << 18;  // pooled entries beyond kInbox, all receivers together
+constexpr uint32_t kNoPost = 0xffffffffu;      // end of a receiver's overflow list
+// The per-scene sums of the sphere gradient run over chunks of this many slots.
+constexpr uint32_t kSumChunk = 8192;
 
 struct AdjArgs {
     AdjStep t;
@@ -52,25 +56,27 @@ struct AdjArgs {
     float *qsc, *lam_part, *lam_extra;
     uint32_t *ccur, *cpred;
     // one-way pair posts: per receiver slot a count and kInbox (sender,
-    // value) entries (entry e of receiver j at e * stride + j), then the
-    // overflow list (receiver, sender, value) with its count
+    // value) entries (entry e of receiver j at e * stride + j); further posts
+    // take pooled entries (sender, value, next) linked from ovf_head[j]
     uint32_t *inbox_count, *inbox_src;
     float4* inbox_val;
-    uint32_t *ovf_count, *ovf_dst, *ovf_src;
+    uint32_t *ovf_head, *ovf_count, *ovf_src, *ovf_next;
     float4* ovf_val;
     // per-slot FP64 accumulators of the scene gradients, reduced per scene in
     // a fixed order: dL/dk (over the whole backward pass) and the sphere's
-    // center (xyz) and radius (w) (over one step)
+    // center (xyz) and radius (w) (over one step, summed per chunk of
+    // kSumChunk slots into spart[scene * sum_chunks + chunk])
     double* kacc;
-    double4* sacc;
+    double4 *sacc, *spart;
+    uint32_t sum_chunks;
     uint32_t* err;                // device error word (kDevErrIndex: a post was dropped)
     double* grads;                // nscenes x kGradStride
 };
 
 // Enqueue the reverse of one step: finalize, every solver iteration in
 // reverse order, predict, and the sphere kinematics.  p_extra, lam_extra,
-// inbox_count and sacc must be zero on entry (they are left zero); kacc
-// accumulates.
+// inbox_count and sacc must be zero and ovf_head kNoPost on entry (they are
+// left so); kacc accumulates.
 cudaError_t launch_adjoint_step(const AdjArgs& a, cudaStream_t s);
 // grads[scene][kGradK] = the sum of kacc over the scene's slots (fixed order);
 // kacc is cleared.
