@@ -81,6 +81,67 @@ def sensitivity(p, dt: float, pos4, vel4, sphere=None, seed: int = 0) -> float:
     return max_abs(a, b)
 
 
+def sensitivity_field(p, dt: float, pos4, vel4, sphere=None, seeds=(0, 1, 2)):
+    """Per-particle conditioning of the FP64 oracle's step at this state: for
+    each seed, every input coordinate is nudged by one FP32 ulp in a random
+    direction and each particle's result is compared with the unperturbed
+    step; kappa_i is the largest move over the seeds.  Returns (the
+    unperturbed oracle output, kappa)."""
+    from oracle import oracle as O
+
+    pos4 = np.asarray(pos4, np.float32)
+    s = None if sphere is None else np.array(sphere, np.float64)
+    base = O.step(p, dt, pos4, vel4, s)
+    kappa = np.zeros(len(pos4))
+    for seed in seeds:
+        rng = np.random.default_rng(seed)
+        pert = pos4.copy()
+        sgn = np.where(rng.random(pert[:, :3].shape) < 0.5, -np.inf, np.inf).astype(np.float32)
+        pert[:, :3] = np.nextafter(pert[:, :3], sgn)
+        s1 = None if sphere is None else np.array(sphere, np.float64)
+        moved = np.abs(O.step(p, dt, pert, vel4, s1)["pos"] - base["pos"]).max(axis=1)
+        kappa = np.maximum(kappa, moved)
+    return base, kappa
+
+
+def neighbourhood_max(values, hashes, dims, reach: int = 2):
+    """For every particle, the largest value over the particles whose hash
+    cells lie within `reach` cells of its own (a (2 reach + 1)^3 block of the
+    grid): a particle's FP32 rounding reaches its neighbours' results, so its
+    own 1-ulp move can understate how far it may go."""
+    from scipy.ndimage import maximum_filter
+
+    dims = [int(d) for d in dims]
+    g = np.zeros(dims[0] * dims[1] * dims[2])
+    hashes = np.asarray(hashes, np.int64)
+    np.maximum.at(g, hashes, values)
+    g = maximum_filter(g.reshape(dims[2], dims[1], dims[0]), size=2 * reach + 1, mode="nearest")
+    return g.ravel()[hashes]
+
+
+def assert_position_distribution(err, kappa_near, frac_floor=None, p99_bound=None,
+                                 ratio_cap: float = 10.0, beyond_frac: float = 1e-3) -> dict:
+    """Checks of an ill-conditioned step, particle by particle and over the
+    distribution (err: per-particle max |GPU - oracle|, kappa_near: the
+    neighbourhood sensitivity):
+      - every particle within ratio_cap x max(1e-5 h, kappa_near_i), and at
+        most a fraction beyond_frac beyond 1 x;
+      - at least frac_floor of the particles within 1e-5 h and the 99th
+        percentile of the error at most p99_bound (when given: measured
+        floors of a workload, which a wrong constant or formula breaks)."""
+    r = err / np.maximum(kappa_near, POS_TOL)
+    stats = {"within_tol": float((err <= POS_TOL).mean()), "p50": float(np.median(err)),
+             "p99": float(np.quantile(err, 0.99)), "max": float(err.max()), "ratio_max": float(r.max()),
+             "beyond_kappa": float((r > 1.0).mean())}
+    assert stats["ratio_max"] <= ratio_cap, f"a particle is {stats['ratio_max']:.1f}x its neighbourhood sensitivity"
+    assert stats["beyond_kappa"] <= beyond_frac, f"{stats['beyond_kappa']:.2e} of particles beyond their sensitivity"
+    if frac_floor is not None:
+        assert stats["within_tol"] >= frac_floor, f"only {stats['within_tol']:.4f} within 1e-5 h (floor {frac_floor})"
+    if p99_bound is not None:
+        assert stats["p99"] <= p99_bound, f"p99 {stats['p99']:.2e} > {p99_bound:.2e}"
+    return stats
+
+
 def position_tolerance(p, dt: float, pos4, vel4, sphere=None) -> float:
     """1e-5 h where the step is well conditioned (a 1-ulp input change moves
     it by less than that); otherwise 4x the measured sensitivity."""
