@@ -346,6 +346,8 @@ StepConsts make_consts(const mp_pbf_params& p, const GridDev& g, uint32_t n, flo
     const float wd = h2 - dq2;
     const float wq = dq2 < h2 ? c.poly6 * wd * wd * wd : 0.0f;
     c.inv_wq = wq > 0.0f ? 1.0f / wq : 0.0f;
+    c.scorr_pq = c.poly6 * c.inv_wq;
+    c.delta_scale = -c.spiky * c.inv_rho0;
     c.max_step = p.max_delta * h;
     c.bminx = p.bounds_min[0];
     c.bminy = p.bounds_min[1];

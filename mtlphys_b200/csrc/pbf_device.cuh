@@ -44,6 +44,8 @@ struct StepConsts {
     float inv_rho0, eps;
     float scorr_k, inv_wq, max_step;
     uint32_t scorr_n;
+    float scorr_pq;     // poly6 / W(dq): s_corr's ratio is d^3 * scorr_pq
+    float delta_scale;  // -spiky / rho0: the position correction's common factor
     float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
     float gravx, gravy, gravz;
     float dt, inv_dt, damping, vmax, vmax_frac;

@@ -262,8 +262,12 @@ struct LambdaAcc {
     }
 };
 
-__device__ __forceinline__ float pow_n_rn(float x, uint32_t n) {
-    if (n == 4u) {
+// ratio^n of s_corr; N = 4 fixes the exponent at compile time (the
+// reference's, Constraints.metal:179), N = 0 takes c.scorr_n.  Both give
+// the same bits for n = 4.
+template <uint32_t N>
+__device__ __forceinline__ float scorr_pow(float x, uint32_t n) {
+    if (N == 4u || (N == 0u && n == 4u)) {
         const float x2 = __fmul_rn(x, x);
         return __fmul_rn(x2, x2);
     }
@@ -272,17 +276,22 @@ __device__ __forceinline__ float pow_n_rn(float x, uint32_t n) {
     return r;
 }
 
-// Position-correction term of one in-range candidate (Constraints.metal:170-181).
+// Position-correction term of one in-range candidate (Constraints.metal:
+// 170-181) with the common factor -spiky / rho0 left out (delta_item
+// applies c.delta_scale once to the sum):
+//   (lambda_i + lambda_j - k (W / W(dq))^n) (h - r)^2 / r  r
+// W / W(dq) = d^3 poly6 / W(dq) (c.scorr_pq); the sum of lambdas and s_corr is
+// one fused multiply-add.
+template <uint32_t N = 0>
 __device__ __forceinline__ void delta_add(const StepConsts& c, float li, float lj, float rx, float ry,
                                           float rz, float r2, float& dx, float& dy, float& dz) {
     if (r2 > 1e-12f) {
         const float d = __fsub_rn(c.h2, r2);
-        const float ratio = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(c.poly6, d), d), d), c.inv_wq);
-        const float scorr = __fmul_rn(-c.scorr_k, pow_n_rn(ratio, c.scorr_n));
+        const float ratio = __fmul_rn(__fmul_rn(__fmul_rn(d, d), d), c.scorr_pq);
         const float rinv = rsqrtf(r2);
         const float hd = fmaxf(__fsub_rn(c.h, __fmul_rn(r2, rinv)), 0.0f);
-        const float coef = __fmul_rn(__fadd_rn(__fadd_rn(li, lj), scorr),
-                                     __fmul_rn(__fmul_rn(__fmul_rn(-c.spiky, hd), hd), rinv));
+        const float coef = __fmul_rn(__fmaf_rn(-c.scorr_k, scorr_pow<N>(ratio, c.scorr_n), __fadd_rn(li, lj)),
+                                     __fmul_rn(__fmul_rn(hd, hd), rinv));
         dx = __fmaf_rn(coef, rx, dx);
         dy = __fmaf_rn(coef, ry, dy);
         dz = __fmaf_rn(coef, rz, dz);
@@ -571,7 +580,8 @@ __device__ __forceinline__ void masked_pairs(const StepConsts& c, const float4* 
 // applyDeltaSorted + sphereCollision on the anchored state; the last
 // iteration also scatters back, finalizes and writes foam.  drec (may be
 // NULL): receives the particle's unclamped correction, for the adjoint.
-template <bool LAST>
+// SN: the s_corr exponent when fixed at compile time (4), else 0.
+template <bool LAST, uint32_t SN = 0>
 __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
                                            const float4* __restrict__ src, float4* __restrict__ dst,
                                            const uint32_t* __restrict__ scell,
@@ -591,7 +601,7 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
     cell_of(c.g, __fadd_rn(ax, l.x), __fadd_rn(ay, l.y), __fadd_rn(az, l.z), cx, cy, cz);
     float dx = 0.0f, dy = 0.0f, dz = 0.0f;
     auto body = [&](uint32_t, const float4& q, float rx, float ry, float rz, float r2) {
-        delta_add(c, l.w, q.w, rx, ry, rz, r2, dx, dy, dz);
+        delta_add<SN>(c, l.w, q.w, rx, ry, rz, r2, dx, dy, dz);
     };
 #ifdef MPB_PARTICLE_OVERFLOW
     if (rm.rows != nullptr && rm.overflow[s] == 0u)
@@ -602,9 +612,9 @@ __device__ __forceinline__ void delta_item(const StepConsts& c, uint32_t s,
     else
         sweep<true>(c, src, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s,
                     static_cast<const RowMasks*>(nullptr), body);
-    dx = __fmul_rn(dx, c.inv_rho0);
-    dy = __fmul_rn(dy, c.inv_rho0);
-    dz = __fmul_rn(dz, c.inv_rho0);
+    dx = __fmul_rn(dx, c.delta_scale);
+    dy = __fmul_rn(dy, c.delta_scale);
+    dz = __fmul_rn(dz, c.delta_scale);
     if (drec) drec[s] = make_float4(dx, dy, dz, 0.0f);
     const float dl = __fsqrt_rn(dist2(dx, dy, dz));
     if (dl > c.max_step) {

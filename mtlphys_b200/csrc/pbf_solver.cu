@@ -57,7 +57,9 @@ k_lambda(StepConsts c, const float4* __restrict__ cur, float4* __restrict__ nxt,
     if (s < c.n) lambda_item<LAST>(c, s, cur, nxt, scell, cstart, sidx, lambdas, rm);
 }
 
-template <bool LAST>
+// SN = 4: the reference's s_corr exponent, fixed at compile time (the host
+// launches this instance when scorr_n == 4); SN = 0 reads it from c.
+template <bool LAST, uint32_t SN>
 __global__ void __launch_bounds__(kSB, (LAST ? MPB_DELTA_MIN_BLOCKS : MPB_DELTA_MID_MIN_BLOCKS) * 256 / kSB)
 k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
         const uint32_t* __restrict__ scell, const uint32_t* __restrict__ cstart,
@@ -66,8 +68,19 @@ k_delta(StepConsts c, const float4* __restrict__ src, float4* __restrict__ dst,
         const uint32_t* __restrict__ ncount, float* __restrict__ foam, uint32_t* err, RowMasks rm) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < c.n)
-        delta_item<LAST>(c, s, src, dst, scell, cstart, sidx, sphere, pos, vel, prev, ncount, foam,
-                         err, rm, nullptr);
+        delta_item<LAST, SN>(c, s, src, dst, scell, cstart, sidx, sphere, pos, vel, prev, ncount, foam,
+                             err, rm, nullptr);
+}
+
+template <bool LAST>
+void launch_delta(const StepConsts& c, const DevState& d, const RowMasks& rm, cudaStream_t s) {
+    const dim3 grid(cdiv(c.n, kSB));
+    if (c.scorr_n == 4)
+        k_delta<LAST, 4><<<grid, kSB, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx, d.sphere,
+                                              d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
+    else
+        k_delta<LAST, 0><<<grid, kSB, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx, d.sphere,
+                                              d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
 }
 
 __global__ void __launch_bounds__(256)
@@ -114,11 +127,9 @@ cudaError_t launch_solver(const StepConsts& c, const DevState& d, uint32_t itera
         tend(t, first ? "lambda_count" : "lambda", s);
         tbegin(t, s);
         if (last)
-            k_delta<true><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
-                                               d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
+            launch_delta<true>(c, d, rm, s);
         else
-            k_delta<false><<<cdiv(n, kSB), kSB, 0, s>>>(c, d.sorted_b, d.sorted_a, d.scell, d.cstart, d.sidx,
-                                                d.sphere, d.pos, d.vel, d.prev, d.ncount, d.foam, d.err, rm);
+            launch_delta<false>(c, d, rm, s);
         tend(t, last ? "delta_finalize" : "delta", s);
     }
     return cudaGetLastError();
