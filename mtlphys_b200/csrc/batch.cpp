@@ -523,6 +523,9 @@ int mp_batch_reset(mp_batch* b, uint32_t nscenes, const uint32_t* counts, const 
         MP_ALLOC(b->scenes, sizeof(SceneDev) * std::max<uint32_t>(nscenes, 1u), b->device);
         a.scenes = b->scenes;
         a.iterations = iters;
+        a.scorr4 = 1;
+        for (uint32_t s = 0; s < nscenes; ++s)
+            if (params[s].scorr_n != 4) a.scorr4 = 0;
         int rc = b->upload_scenes();
         if (rc != MP_OK) return rc;
         if (total) {
@@ -802,6 +805,9 @@ int mp_batch_set_params(mp_batch* b, uint32_t scene, const mp_pbf_params* params
                         b->scene_ids[scene] == MP_SCENE_SPHERE_DROP);
     MP_CUDA(cudaMemcpy(&b->scenes[scene], &cur, sizeof(SceneDev), cudaMemcpyHostToDevice));
     b->params[scene] = *params;
+    b->a.scorr4 = 1;
+    for (const mp_pbf_params& q : b->params)
+        if (q.scorr_n != 4) b->a.scorr4 = 0;
     b->host_scenes[scene].c = cur.c;
     b->drop_graph();
     return MP_OK;

@@ -117,7 +117,9 @@ constexpr int batch_min_blocks() {
     return int(65536u / (BS * 64u));
 }
 
-template <uint32_t BS>
+// SN: the s_corr exponent fixed at compile time (4, when every scene uses
+// the reference's) or read per scene (0); both give the same bits for 4.
+template <uint32_t BS, uint32_t SN>
 __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(BatchArgs a) {
     __shared__ uint32_t s_warp[BS / 32 + 1];
     __shared__ int s_ok;
@@ -342,10 +344,10 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
         for (uint32_t s = pb + gtid; s < pe; s += gsize) {
             const SceneDev& sd = sc[a.scene_of[s]];
             if (last)
-                delta_item<true>(sd.c, s, lam_out, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
+                delta_item<true, SN>(sd.c, s, lam_out, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
                                  a.pos, a.vel, a.prev, a.ncount, a.foam, a.err, rmi, drec);
             else
-                delta_item<false>(sd.c, s, lam_out, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
+                delta_item<false, SN>(sd.c, s, lam_out, a.sorted_a, a.scell, a.cstart, a.sidx, &sd.sphere,
                                   a.pos, a.vel, a.prev, a.ncount, a.foam, a.err, rmi, drec);
         }
         if (!last && !grid_barrier(a, &s_ok)) return;
@@ -355,16 +357,19 @@ __global__ void __launch_bounds__(BS, batch_min_blocks<BS>()) k_batch_step(Batch
 template <uint32_t BS>
 cudaError_t launch_bs(const BatchArgs& args, uint32_t blocks, cudaStream_t s) {
     void* kargs[] = {const_cast<BatchArgs*>(&args)};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&k_batch_step<BS>), dim3(blocks),
-                                       dim3(BS), kargs, 0, s);
+    const void* fn = args.scorr4 ? reinterpret_cast<const void*>(&k_batch_step<BS, 4>)
+                                 : reinterpret_cast<const void*>(&k_batch_step<BS, 0>);
+    return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(BS), kargs, 0, s);
 }
 
+// Blocks of both instances that fit on one SM at once (the smaller count).
 template <uint32_t BS>
 int occupancy_bs() {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_step<BS>, BS, 0) != cudaSuccess)
+    int n0 = 0, n4 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k_batch_step<BS, 0>, BS, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n4, k_batch_step<BS, 4>, BS, 0) != cudaSuccess)
         return 0;
-    return n;
+    return n0 < n4 ? n0 : n4;
 }
 
 }  // namespace

@@ -57,6 +57,7 @@ struct BatchArgs {
     // many more blocks than the launch has, so that each wait runs out.
     uint32_t* abort;
     uint32_t spin_limit, bar_extra;
+    uint32_t scorr4;  // 1: every scene's s_corr exponent is 4 (the kernel fixes it at compile time)
     BatchRecord rec;
 };
 
