@@ -100,7 +100,9 @@ template <bool VEC>
 __global__ void __launch_bounds__(kScanThreads)
 k_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status,
        unsigned long long* ticket, uint32_t tiles, int zero_input, uint32_t* err, uint32_t spin_limit) {
-    __shared__ uint32_t s_tile, s_tag, s_warp[kScanThreads / 32], s_excl;
+    constexpr uint32_t kScanWarps = kScanThreads / 32;
+    __shared__ uint32_t s_tile, s_tag, s_warp[kScanWarps], s_agg, s_fail;
+    __shared__ uint32_t s_has[kScanWarps], s_sum[kScanWarps];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
         const unsigned long long t = atomicAdd(ticket, 1ull);
@@ -112,11 +114,12 @@ k_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status
     const uint32_t wbase = tile * kScanTile + warp * 512u;
 
     uint32_t v[4][4], pre[4];
+    // all four loads in flight before the first shuffle
+#pragma unroll
+    for (int k = 0; k < 4; ++k) load4<VEC>(in, wbase + k * 128u + lane * 4u, n, v[k]);
     uint32_t running = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const uint32_t idx = wbase + k * 128u + lane * 4u;
-        load4<VEC>(in, idx, n, v[k]);
         const uint32_t t = v[k][0] + v[k][1] + v[k][2] + v[k][3];
         uint32_t incl = t;
 #pragma unroll
@@ -136,55 +139,79 @@ k_scan(const uint32_t* in, uint32_t* out, uint32_t n, unsigned long long* status
     __syncthreads();
 
     if (warp == 0) {
-        // Block-level scan of the 8 warp totals.
-        const uint32_t wt = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+        // Block-level scan of the 8 warp totals; publish the tile aggregate
+        // (tile 0: its inclusive prefix).
+        const uint32_t wt = lane < kScanWarps ? s_warp[lane] : 0u;
         uint32_t wincl = wt;
 #pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
+        for (int o = 1; o < int(kScanWarps); o <<= 1) {
             const uint32_t y = __shfl_up_sync(kFull, wincl, o);
             if (lane >= uint32_t(o)) wincl += y;
         }
-        const uint32_t agg = __shfl_sync(kFull, wincl, kScanThreads / 32 - 1);
-        if (lane < kScanThreads / 32) s_warp[lane] = wincl - wt;
-
-        uint32_t excl = 0;
-        if (tile == 0) {
-            if (lane == 0) *(volatile unsigned long long*)&status[0] = pack_status(tag, 1u, agg);
-        } else {
-            if (lane == 0) *(volatile unsigned long long*)&status[tile] = pack_status(tag, 0u, agg);
-            int base = int(tile) - 1;
-            uint32_t spins = 0;
-            while (true) {
-                const int idx = base - int(lane);
-                const unsigned long long w =
-                    idx >= 0 ? *(volatile unsigned long long*)&status[idx] : pack_status(tag, 1u, 0u);
-                const bool valid = uint32_t(w >> 33) == tag;
-                if (__all_sync(kFull, valid)) {
-                    const unsigned pm = __ballot_sync(kFull, ((w >> 32) & 1ull) != 0ull);
-                    uint32_t val = uint32_t(w);
-                    if (pm) {
-                        const int first = __ffs(pm) - 1;
-                        if (int(lane) > first) val = 0;
-                        excl += warp_sum(val);
-                        break;
-                    }
-                    excl += warp_sum(val);
-                    base -= 32;
-                } else {
-                    if (++spins > spin_limit) {
-                        if (lane == 0) atomicOr(err, kDevErrSpin);
-                        break;
-                    }
-                    __nanosleep(32);
-                }
-            }
-            if (lane == 0) *(volatile unsigned long long*)&status[tile] = pack_status(tag, 1u, excl + agg);
+        const uint32_t agg = __shfl_sync(kFull, wincl, kScanWarps - 1);
+        if (lane < kScanWarps) s_warp[lane] = wincl - wt;
+        if (lane == 0) {
+            s_agg = agg;
+            s_fail = 0;
+            *(volatile unsigned long long*)&status[tile] = pack_status(tag, tile == 0 ? 1u : 0u, agg);
         }
-        if (lane == 0) s_excl = excl;
     }
     __syncthreads();
 
-    const uint32_t tile_excl = s_excl + s_warp[warp];
+    // Look-back by all warps at once: warp w polls the 32 descriptors
+    // [base - 32w - 31, base - 32w] until each holds at least an aggregate of
+    // this epoch; the nearest inclusive prefix among the 256 ends the walk,
+    // else their aggregates are summed and the next 256 follow.  A window
+    // that stays stale past the spin limit flags the error word and ends the
+    // walk with the prefix summed so far.
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int base = int(tile) - 1;
+        uint32_t spins = 0;
+        bool done = false;
+        while (!done) {
+            const int idx = base - int(warp * 32u + lane);
+            unsigned long long w;
+            bool valid;
+            while (true) {
+                w = idx >= 0 ? *(volatile unsigned long long*)&status[idx] : pack_status(tag, 1u, 0u);
+                valid = uint32_t(w >> 33) == tag;
+                if (__all_sync(kFull, valid)) break;
+                if (++spins > spin_limit) break;
+                __nanosleep(32);
+            }
+            const bool ok = __all_sync(kFull, valid);
+            const unsigned incl = __ballot_sync(kFull, ((w >> 32) & 1ull) != 0ull);
+            const uint32_t val = uint32_t(w);
+            const int first = incl ? __ffs(incl) - 1 : 32;
+            const uint32_t nearest = warp_sum(int(lane) <= first ? val : 0u);
+            if (lane == 0) {
+                if (!ok) {
+                    atomicOr(err, kDevErrSpin);
+                    s_fail = 1;
+                }
+                s_has[warp] = incl != 0u;
+                s_sum[warp] = nearest;
+            }
+            __syncthreads();
+            if (s_fail) {
+                done = true;
+            } else {
+                uint32_t acc = 0;
+                for (uint32_t q = 0; q < kScanWarps && !done; ++q) {
+                    acc += s_sum[q];
+                    done = s_has[q] != 0u;
+                }
+                excl += acc;
+                base -= int(kScanThreads);
+                done = done || base < 0;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) *(volatile unsigned long long*)&status[tile] = pack_status(tag, 1u, excl + s_agg);
+    }
+
+    const uint32_t tile_excl = excl + s_warp[warp];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         uint32_t o[4];
