@@ -201,7 +201,9 @@ typedef struct mp_kernel_time {
     double   ms;         /* total device time of those launches           */
 } mp_kernel_time;
 /* Time every kernel the engine launches with CUDA events on its stream
- * (1), or stop (0).  While profiling, step() runs kernel by kernel. */
+ * (1), or stop (0).  While profiling, step() runs kernel by kernel, or, in
+ * graph mode, as one graph captured with the timing events as event nodes
+ * (instantiated per step; the times then exclude the host's launch gaps). */
 int mp_engine_set_profiling(mp_engine* e, int enable);
 /* Wait for the timed work and return per-kernel totals (up to `capacity`
  * entries; *count = number of kernel kinds); the totals are then cleared. */

@@ -402,14 +402,35 @@ struct EventTimer final : mpb::KernelTimer {
         }
         return pool[used++];
     }
+    // graphs of profiled steps, kept until their events are read
+    std::vector<std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+
+    // Under stream capture the record becomes an event node of the graph
+    // (cudaEventRecordExternal), so the events time the kernels as the graph
+    // runs them, without the host's launch gaps between them.
+    static void record(cudaEvent_t ev, cudaStream_t s) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+            cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal);
+        else
+            cudaEventRecord(ev, s);
+    }
     void begin(cudaStream_t s) override {
         open = used;
-        cudaEventRecord(next(), s);
+        record(next(), s);
     }
     void end(const char* kernel, cudaStream_t s) override {
         const size_t e = used;
-        cudaEventRecord(next(), s);
+        record(next(), s);
         marks.push_back({kernel, open, e});
+    }
+    void release_graphs() {
+        if (!graphs.empty()) cudaDeviceSynchronize();
+        for (auto& g : graphs) {
+            if (g.second) cudaGraphExecDestroy(g.second);
+            if (g.first) cudaGraphDestroy(g.first);
+        }
+        graphs.clear();
     }
     cudaError_t collect() {
         for (const Mark& m : marks) {
@@ -423,9 +444,11 @@ struct EventTimer final : mpb::KernelTimer {
         }
         marks.clear();
         used = 0;
+        release_graphs();
         return status;
     }
     ~EventTimer() override {
+        release_graphs();
         for (cudaEvent_t ev : pool)
             if (ev) cudaEventDestroy(ev);
     }
@@ -765,7 +788,28 @@ int mp_engine_step(mp_engine* e, float dt, mp_stream stream) {
             const cudaError_t ce = e->timer->collect();
             if (ce != cudaSuccess) return fail(MP_ERR_CUDA, "profiling: %s", cudaGetErrorString(ce));
         }
-        return e->enqueue_step(dt, s, e->timer);
+        if (!e->graph_mode) return e->enqueue_step(dt, s, e->timer);
+        // graph mode: the step and its timing events captured as one graph
+        // (instantiated per step, released when the times are read)
+        if (!e->cap_stream) MP_CUDA(cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking));
+        MP_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = e->enqueue_step(dt, e->cap_stream, e->timer);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &graph);
+        if (rc != MP_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(MP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        if (ie != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return fail(MP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+        }
+        e->timer->graphs.push_back({graph, exec});
+        MP_CUDA(cudaGraphLaunch(exec, s));
+        return MP_OK;
     }
     if (!e->graph_mode) return e->enqueue_step(dt, s);
     if (!e->gexec || e->graph_dt != dt || e->graph_spin_epoch != mpb::spin_limit_epoch()) {

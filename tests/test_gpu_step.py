@@ -447,3 +447,29 @@ def test_full_length_runs_stay_valid(eng, workload):
     assert np.array_equal(hs[si], cell_of_slot)
     same = cell_of_slot[1:] == cell_of_slot[:-1]
     assert (si[1:][same] > si[:-1][same]).all()
+
+
+def test_profiling_in_graph_mode_times_every_kernel_and_keeps_the_bits(eng):
+    """Per-kernel timing captured with the step's graph (event nodes) times
+    each launch of the step and gives the same state as an untimed step."""
+    w = configs.cube_drop(side=24)
+    k = int(w.params.solver_iterations)
+    outs = []
+    for profile in (False, True):
+        eng.set_params(w.params)
+        eng.reset(w.n, w.scene, w.desc)
+        eng.set_graph_mode(True)
+        eng.set_profiling(profile)
+        for _ in range(4):
+            eng.step(w.dt)
+        if profile:
+            times = eng.kernel_times()
+            launches = sum(v[0] for v in times.values())
+            assert launches == 4 * int(_abi.load().mp_step_launch_count(k)), times
+            assert all(v[1] > 0.0 for v in times.values()), times
+            assert times["lambda_count"][0] == 4 and times["delta_finalize"][0] == 4
+            eng.set_profiling(False)
+        assert eng.check_errors() == 0
+        outs.append((eng.positions(), eng.velocities()))
+        eng.set_graph_mode(False)
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
