@@ -257,6 +257,7 @@ def run_ours(args, world, rank, local) -> dict | None:
     _abi.check(lib.mp_engine_download(e._h, _abi.MP_BUF_POSITIONS, C.c_void_p(h_pos.data_ptr()), n, sh), "download")
     _abi.check(lib.mp_engine_download(e._h, _abi.MP_BUF_VELOCITIES, C.c_void_p(h_vel.data_ptr()), n, sh), "download")
     stream.synchronize()
+    start_state = (h_pos.numpy().copy(), h_vel.numpy().copy())  # for the CPU baseline
 
     # ---- timed region: K steps, L2 flushed between steps (outside the events)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -417,7 +418,7 @@ def run_ours(args, world, rank, local) -> dict | None:
         line["adjoint"] = adjoint
         line["gpu_launches"] += adjoint.pop("launches_timed")
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, args)
+        line["cpu_baseline"] = cpu_baseline(w, args, start_state, args.warmup)
     return line
 
 
@@ -642,14 +643,14 @@ def read_traffic(kernel: str):
     return None
 
 
-def cpu_baseline(w, args) -> dict:
-    """The FP64 oracle on the host cores, a bounded sample of the workload."""
+def cpu_baseline(w, args, start, first_step) -> dict:
+    """The FP64 oracle on the host cores, a bounded sample of the workload:
+    the first of the timed region's steps, from its start state."""
     import numpy as np
 
     from oracle import oracle as O
 
-    pos = O.seed_scene(w.params, w.scene, w.n, w.desc)
-    vel = np.zeros_like(pos)
+    pos, vel = start
     O.set_threads(0)
     steps = 0
     t0 = time.perf_counter()
@@ -661,7 +662,8 @@ def cpu_baseline(w, args) -> dict:
     dt = time.perf_counter() - t0
     return {"value": round(dt * 1000.0 / steps, 2), "unit": "ms/step", "cores": O.threads(),
             "kind": "port",
-            "sample": f"first {steps} steps of the {w.name} workload ({w.n} particles), FP64 oracle"}
+            "sample": f"steps {first_step}-{first_step + steps - 1} of the {w.name} workload ({w.n} particles; "
+                      f"the first {steps} timed steps, from their start state), FP64 oracle"}
 
 
 # ---- reference arm ----------------------------------------------------------------------
@@ -812,7 +814,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["dam_break", "cube_drop"], default="dam_break")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=15)
     ap.add_argument("--cpu-budget-s", type=float, default=60.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched leg")
