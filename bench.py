@@ -745,6 +745,8 @@ def run_profile(which: str) -> str:
     """One workload run once, a short fixed sequence of launches for a
     profiler to capture: `step` (1M dam break, 3 steps), `batch` (256 cube
     drops, 3 batched steps), `adjoint` (97K cube, 20-step rollout + gradient),
+    `adjoint_spheres` (32 sphere drops, 10-step rollout + gradient; `_small`:
+    4 of them, for captures that save and restore device memory),
     `render` (1M dam break, 3 frames at 1280x720).  Returns one line with its
     CUDA-event time; not a benchmark value."""
     import torch
@@ -791,6 +793,21 @@ def run_profile(which: str) -> str:
         ms = timed(go)
         b.check_errors()
         return f"adjoint: {w.steps}-step rollout + gradient of {w.n} particles in {ms:.3f} ms"
+    if which in ("adjoint_spheres", "adjoint_spheres_small"):
+        w = configs.batch_spheres(num=32 if which == "adjoint_spheres" else 4, steps=10)
+        b = Batch(0)
+        b.reset(w.counts, w.params, w.dts, w.scenes, w.descs)
+        g = torch.zeros((w.n, 4), device="cuda")
+        g[:, 1] = 1.0 / w.n
+
+        def go():
+            b.rollout_forward(w.steps, 10, stream)
+            b.rollout_backward(g, None, stream)
+
+        ms = timed(go)
+        b.check_errors()
+        return (f"{which}: {w.steps}-step rollout + gradient of {len(w.counts)} scenes "
+                f"({w.n} particles) in {ms:.3f} ms")
     if which == "render":
         w = configs.dam_break()
         e = Engine(0)
@@ -819,7 +836,7 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--batch-steps", type=int, default=10, help="timed steps of the batched leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
-    ap.add_argument("--profile", choices=["step", "batch", "adjoint", "render"],
+    ap.add_argument("--profile", choices=["step", "batch", "adjoint", "adjoint_spheres", "adjoint_spheres_small", "render"],
                     help="run one fixed short workload for a profiler and exit (no bench line)")
     args = ap.parse_args()
     if args.profile:

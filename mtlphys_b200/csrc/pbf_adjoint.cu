@@ -107,12 +107,15 @@ __device__ __forceinline__ void post(const AdjArgs& a, uint32_t to, uint32_t fro
 __global__ void __launch_bounds__(kBlock) k_adj_finalize(AdjArgs a) {
     const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
     if (s >= a.n) return;
-    const StepConsts& c = a.t.scenes[a.scene_of[s]].c;
+    // loads first (in flight together), stores after
+    const uint32_t sc = __ldg(&a.scene_of[s]);
+    const uint32_t cell = __ldg(&a.t.scell[s]);
+    const uint32_t j = __ldg(&a.t.sidx[s]);
+    const float4 X4 = __ldg(&a.t.x1[j]), P4 = __ldg(&a.t.x0[j]), xb = a.xbar[j], vb = a.vbar[j];
+    const StepConsts& c = a.t.scenes[sc].c;
     int px, py, pz;
-    decode_cell(c.g, a.t.scell[s], px, py, pz);
+    decode_cell(c.g, cell, px, py, pz);
     a.cpred[s] = pack_cell(px + c.g.lx, py + c.g.ly, pz + c.g.lz);
-    const uint32_t j = a.t.sidx[s];
-    const float4 X4 = a.t.x1[j], P4 = a.t.x0[j], xb = a.xbar[j], vb = a.vbar[j];
     const double X[3] = {X4.x, X4.y, X4.z}, P[3] = {P4.x, P4.y, P4.z};
     const double lo_b[3] = {c.bminx, c.bminy, c.bminz}, hi_b[3] = {c.bmaxx, c.bmaxy, c.bmaxz};
     const double kd = double(c.damping) / double(c.dt);
@@ -153,13 +156,18 @@ __global__ void __launch_bounds__(kBlock) k_adj_pre(AdjArgs a, uint32_t it) {
     const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
     if (s == 0) *a.ovf_count = 0;  // the delta sweep posts into an empty list
     if (s >= a.n) return;
-    const SceneDev& sd = a.t.scenes[a.scene_of[s]];
-    const StepConsts& c = sd.c;
+    // every per-slot input first, so their loads are in flight together
     const size_t off = size_t(it) * a.stride;
-    const float4 l = a.t.lam[off + s];
-    const float4 dr = a.t.delta[off + s];
+    const uint32_t sc = __ldg(&a.scene_of[s]);
+    const float4 l = __ldg(&a.t.lam[off + s]);
+    const float4 dr = __ldg(&a.t.delta[off + s]);
+    const uint32_t cell = __ldg(&a.t.scell[s]);
+    const float4 pe = a.p_extra[s];
+    const float4 pb4 = a.pbar[s];
+    const SceneDev& sd = a.t.scenes[sc];
+    const StepConsts& c = sd.c;
     int pcx, pcy, pcz;
-    decode_cell(c.g, a.t.scell[s], pcx, pcy, pcz);
+    decode_cell(c.g, cell, pcx, pcy, pcz);
     const float ax = anchor_x(c.g, pcx), ay = anchor_y(c.g, pcy), az = anchor_z(c.g, pcz);
     int cx, cy, cz;
     cell_of(c.g, __fadd_rn(ax, l.x), __fadd_rn(ay, l.y), __fadd_rn(az, l.z), cx, cy, cz);
@@ -183,8 +191,6 @@ __global__ void __launch_bounds__(kBlock) k_adj_pre(AdjArgs a, uint32_t it) {
         qc[k] = fmin(fmax(q[k], lo_b[k]), hi_b[k]);
     }
 
-    const float4 pe = a.p_extra[s];
-    const float4 pb4 = a.pbar[s];
     a.p_extra[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float pb[3] = {pb4.x + pe.x, pb4.y + pe.y, pb4.z + pe.z};
     if (c.sphere) {
@@ -458,14 +464,28 @@ __global__ void __launch_bounds__(kBlock) k_adj_sphere_sum(AdjArgs a) {
     if (!sd.c.sphere) return;  // only sphere scenes accumulate
     const uint32_t first = chunk * kSumChunk, n = sd.c.n;
     const uint32_t end = min(n, first + kSumChunk);
+    // kSumChunk / kBlock = 8 entries per thread, loaded 4 at a time before
+    // they are added (in index order) and cleared
+    static_assert(kSumChunk == 8 * kBlock, "two rounds of four loads per thread");
     double cx = 0.0, cy = 0.0, cz = 0.0, r = 0.0;
-    for (uint32_t i = first + threadIdx.x; i < end; i += kBlock) {
-        const double4 v = a.sacc[sd.p0 + i];
-        cx += v.x;
-        cy += v.y;
-        cz += v.z;
-        r += v.w;
-        a.sacc[sd.p0 + i] = make_double4(0.0, 0.0, 0.0, 0.0);
+    double4* acc = a.sacc + sd.p0;
+#pragma unroll
+    for (uint32_t round = 0; round < 2; ++round) {
+        double4 v[4];
+#pragma unroll
+        for (uint32_t u = 0; u < 4; ++u) {
+            const uint32_t i = first + (round * 4 + u) * kBlock + threadIdx.x;
+            v[u] = i < end ? acc[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < 4; ++u) {
+            const uint32_t i = first + (round * 4 + u) * kBlock + threadIdx.x;
+            cx += v[u].x;
+            cy += v[u].y;
+            cz += v[u].z;
+            r += v[u].w;
+            if (i < end) acc[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        }
     }
     cx = block_sum(cx, sh);
     cy = block_sum(cy, sh);
@@ -494,14 +514,16 @@ __global__ void __launch_bounds__(kBlock) k_adj_k_sum(AdjArgs a) {
 __global__ void __launch_bounds__(kBlock) k_adj_predict(AdjArgs a) {
     const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
     if (s >= a.n) return;
-    const StepConsts& c = a.t.scenes[a.scene_of[s]].c;
+    // loads first (in flight together), stores after
+    const uint32_t sc = __ldg(&a.scene_of[s]);
+    const uint32_t j = __ldg(&a.t.sidx[s]);
     const float4 pb = a.pbar[s], pe = a.p_extra[s];
+    const float4 xb = a.xbar[j];
+    const float dt = a.t.scenes[sc].c.dt;
     a.p_extra[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float bx = pb.x + pe.x, by = pb.y + pe.y, bz = pb.z + pe.z;
-    const uint32_t j = a.t.sidx[s];
-    const float4 xb = a.xbar[j];
     a.xbar[j] = make_float4(xb.x + bx, xb.y + by, xb.z + bz, 0.0f);
-    a.vbar[j] = make_float4(bx * c.dt, by * c.dt, bz * c.dt, 0.0f);
+    a.vbar[j] = make_float4(bx * dt, by * dt, bz * dt, 0.0f);
 }
 
 // The sphere's kinematic advance of this step (sphere_advance) reversed:
@@ -512,15 +534,30 @@ __global__ void __launch_bounds__(128) k_adj_sphere(AdjArgs a) {
     const StepConsts& c = a.t.scenes[sc].c;
     if (!c.sphere) return;
     {  // this step's push terms, chunk by chunk in order (k_adj_sphere_sum)
+        // added in chunk order in registers (the same sums as adding each
+        // chunk into g), loads four chunks ahead
         double* g = a.grads + size_t(sc) * kGradStride;
         const uint32_t chunks = (c.n + kSumChunk - 1) / kSumChunk;
-        for (uint32_t k = 0; k < chunks; ++k) {
-            const double4 v = a.spart[size_t(sc) * a.sum_chunks + k];
-            g[kGradCenter] += v.x;
-            g[kGradCenter + 1] += v.y;
-            g[kGradCenter + 2] += v.z;
-            g[kGradRadius] += v.w;
+        const double4* part = a.spart + size_t(sc) * a.sum_chunks;
+        double gx = g[kGradCenter], gy = g[kGradCenter + 1], gz = g[kGradCenter + 2], gr = g[kGradRadius];
+        for (uint32_t k0 = 0; k0 < chunks; k0 += 4) {
+            double4 v[4];
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u)
+                v[u] = k0 + u < chunks ? part[k0 + u] : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+            for (uint32_t u = 0; u < 4; ++u) {
+                if (k0 + u >= chunks) break;
+                gx += v[u].x;
+                gy += v[u].y;
+                gz += v[u].z;
+                gr += v[u].w;
+            }
         }
+        g[kGradCenter] = gx;
+        g[kGradCenter + 1] = gy;
+        g[kGradCenter + 2] = gz;
+        g[kGradRadius] = gr;
     }
     const SphereState s0 = a.t.sphere0[sc];
     // forward branch decisions, as sphere_advance computes them

@@ -43,7 +43,7 @@ constexpr uint32_t kInbox = 4;
 constexpr uint32_t kInboxOverflow = 1u << 18;  // pooled entries beyond kInbox, all receivers together
 constexpr uint32_t kNoPost = 0xffffffffu;      // end of a receiver's overflow list
 // The per-scene sums of the sphere gradient run over chunks of this many slots.
-constexpr uint32_t kSumChunk = 8192;
+constexpr uint32_t kSumChunk = 2048;
 
 struct AdjArgs {
     AdjStep t;
