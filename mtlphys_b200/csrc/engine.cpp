@@ -792,19 +792,31 @@ int mp_engine_step(mp_engine* e, float dt, mp_stream stream) {
         // graph mode: the step and its timing events captured as one graph
         // (instantiated per step, released when the times are read)
         if (!e->cap_stream) MP_CUDA(cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking));
+        // a step that does not run leaves no marks behind (their events are
+        // never recorded)
+        const size_t marks0 = e->timer->marks.size(), used0 = e->timer->used;
+        auto forget = [&] {
+            e->timer->marks.resize(marks0);
+            e->timer->used = used0;
+        };
         MP_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
         const int rc = e->enqueue_step(dt, e->cap_stream, e->timer);
         cudaGraph_t graph = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &graph);
         if (rc != MP_OK) {
             if (graph) cudaGraphDestroy(graph);
+            forget();
             return rc;
         }
-        if (ce != cudaSuccess) return fail(MP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        if (ce != cudaSuccess) {
+            forget();
+            return fail(MP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        }
         cudaGraphExec_t exec = nullptr;
         const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         if (ie != cudaSuccess) {
             cudaGraphDestroy(graph);
+            forget();
             return fail(MP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
         }
         e->timer->graphs.push_back({graph, exec});
