@@ -42,15 +42,16 @@ def shard_workload(w, rank: int, world: int):
 def gather_scene_scalars(values, idx, nscenes: int, world: int):
     """All-gather per-scene FP64 scalars (one value per scene this rank owns,
     scene indices `idx`) into a length-`nscenes` list on every rank.  Uses
-    the default process group (NCCL on GPUs, gloo on CPU) when world > 1."""
+    the default process group (NCCL on GPUs, gloo on CPU) when one is
+    initialised, a single rank included; without one, world must be 1."""
     import torch
+    import torch.distributed as dist
 
     out = [0.0] * nscenes
-    if world == 1:
+    if world == 1 and not (dist.is_available() and dist.is_initialized()):
         for i, v in zip(idx, values):
             out[i] = float(v)
         return out
-    import torch.distributed as dist
 
     dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
     local = torch.zeros(nscenes, dtype=torch.float64, device=dev)

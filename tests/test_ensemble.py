@@ -70,3 +70,7 @@ def test_gather_scene_scalars_over_two_gloo_ranks(tmp_path):
     want = np.array([1000.0 * s + 0.125 for s in range(len(counts))])
     for r in range(2):
         np.testing.assert_array_equal(np.load(tmp_path / f"r{r}.npy"), want)
+
+
+def test_gather_scene_scalars_without_a_process_group():
+    assert gather_scene_scalars([2.5, -1.0], [2, 0], 3, 1) == [-1.0, 0.0, 2.5]
