@@ -383,6 +383,8 @@ __device__ __forceinline__ uint32_t sweep(const StepConsts& c, const float4* __r
                 }
                 if (c0 == b0) first = mask;
                 hits += __popc(mask);
+                // the particle's own slot gets no body (its r is 0)
+                if (s - c0 < 32u) mask &= ~(1u << (s - c0));
                 while (mask) {
                     const uint32_t k = c0 + uint32_t(__ffs(mask) - 1);
                     mask &= mask - 1;
@@ -427,7 +429,7 @@ __device__ __forceinline__ void lambda_first_item(const StepConsts& c, uint32_t 
                                       rm.rows ? &rm : nullptr,
                                       [&](uint32_t k, const float4&, float rx, float ry, float rz,
                                           float r2) {
-                                          if (k != s) acc.add(c, rx, ry, rz, r2);
+                                          acc.add(c, rx, ry, rz, r2);
                                       });
     const float lambda = acc.lambda(c);
     // l = p - A(c): exact for the particle's own cell (Sterbenz) unless the
@@ -463,7 +465,7 @@ __device__ __forceinline__ void lambda_item(const StepConsts& c, uint32_t s,
     acc.self(c);
     sweep<true, true>(c, cur, cstart, cx, cy, cz, l.x, l.y, l.z, pcx, pcy, pcz, s, rm.rows ? &rm : nullptr,
                       [&](uint32_t k, const float4&, float rx, float ry, float rz, float r2) {
-                          if (k != s) acc.add(c, rx, ry, rz, r2);
+                          acc.add(c, rx, ry, rz, r2);
                       });
     const float lambda = acc.lambda(c);
     nxt[s] = make_float4(l.x, l.y, l.z, lambda);
