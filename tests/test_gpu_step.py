@@ -449,16 +449,18 @@ def test_full_length_runs_stay_valid(eng, workload):
     assert (si[1:][same] > si[:-1][same]).all()
 
 
-def test_profiling_in_graph_mode_times_every_kernel_and_keeps_the_bits(eng):
-    """Per-kernel timing captured with the step's graph (event nodes) times
-    each launch of the step and gives the same state as an untimed step."""
+@pytest.mark.parametrize("graph", [True, False])
+def test_profiling_times_every_kernel_and_keeps_the_bits(eng, graph):
+    """Per-kernel timing, kernel by kernel or captured with the step's graph
+    (event nodes), times each launch of the step and gives the same state as
+    an untimed step."""
     w = configs.cube_drop(side=24)
     k = int(w.params.solver_iterations)
     outs = []
     for profile in (False, True):
         eng.set_params(w.params)
         eng.reset(w.n, w.scene, w.desc)
-        eng.set_graph_mode(True)
+        eng.set_graph_mode(graph)
         eng.set_profiling(profile)
         for _ in range(4):
             eng.step(w.dt)
